@@ -1,0 +1,1103 @@
+// C ABI of libadabool (include/adabool.h): index lifecycle, reference-shaped
+// workers (prepare + run into a caller bitmap), the native batch runner and
+// the single-query convenience call.
+#include "abf_kernels.cuh"
+
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <exception>
+#include <new>
+#include <string>
+
+namespace {
+thread_local std::string g_err;
+std::atomic<uint64_t> g_launches{0};
+}  // namespace
+
+namespace abf {
+abf_status fail(abf_status s, const std::string& msg) {
+    g_err = msg;
+    return s;
+}
+void clear_error() { g_err.clear(); }
+void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+}  // namespace abf
+
+using abf::fail;
+
+#define CUDA_TRY(expr)                                                                                   \
+    do {                                                                                                 \
+        cudaError_t e_ = (expr);                                                                         \
+        if (e_ != cudaSuccess)                                                                           \
+            return fail(e_ == cudaErrorMemoryAllocation ? ABF_ERR_OOM : ABF_ERR_CUDA,                    \
+                        std::string(#expr) + ": " + cudaGetErrorString(e_));                             \
+    } while (0)
+
+#define ABF_TRY(expr)                      \
+    do {                                   \
+        abf_status s_ = (expr);            \
+        if (s_ != ABF_OK) return s_;       \
+    } while (0)
+
+#define API_BEGIN try {
+#define API_END                                                                 \
+    }                                                                           \
+    catch (const std::bad_alloc&) {                                             \
+        return fail(ABF_ERR_OOM, "host allocation failed");                     \
+    }                                                                           \
+    catch (const std::exception& ex) {                                          \
+        return fail(ABF_ERR_INTERNAL, ex.what());                               \
+    }                                                                           \
+    catch (...) {                                                               \
+        return fail(ABF_ERR_INTERNAL, "unknown exception");                     \
+    }
+
+namespace {
+
+// ---- kernel timing (abf_profile_enable / abf_profile_read) ----
+enum Kid { K_PLAN, K_QUEUE, K_PROBE_BITS, K_TILE, K_SCATTER, K_PROBE, K_COUNT, K_SCAN, K_WRITE, K_NKERNELS };
+const char* const kKernelNames[K_NKERNELS] = {"plan",   "queue_scan",    "probe_bits",   "tile_union",
+                                              "scatter_union", "probe", "compact_count", "compact_scan",
+                                              "compact_write"};
+
+struct Profiler {
+    struct Rec {
+        int kid;
+        cudaEvent_t a, b;
+    };
+    std::vector<cudaEvent_t> pool;
+    std::vector<Rec> recs;
+    cudaEvent_t get() {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    ~Profiler() {
+        for (auto& r : recs) {
+            cudaEventDestroy(r.a);
+            cudaEventDestroy(r.b);
+        }
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
+
+// Records an event pair around one launch when timing is on.
+struct ProfScope {
+    abf_index* ix;
+    int kid;
+    cudaStream_t s;
+    cudaEvent_t a = nullptr;
+    ProfScope(abf_index* ix_, int kid_, cudaStream_t s_) : ix(ix_), kid(kid_), s(s_) {
+        if (ix->prof_on && ix->prof) {
+            a = static_cast<Profiler*>(ix->prof)->get();
+            cudaEventRecord(a, s);
+        }
+    }
+    ~ProfScope() {
+        if (a) {
+            auto* p = static_cast<Profiler*>(ix->prof);
+            cudaEvent_t b = p->get();
+            cudaEventRecord(b, s);
+            p->recs.push_back({kid, a, b});
+        }
+    }
+};
+
+}  // namespace
+
+#define TIMED(kid, expr)                \
+    do {                                \
+        ProfScope ps_(ix, (kid), s);    \
+        CUDA_TRY(expr);                 \
+    } while (0)
+
+struct abf_workspace {
+    abf_index* ix = nullptr;
+    uint32_t max_q = 0;
+    uint64_t max_terms = 0;
+    uint32_t probe_cap = 0;
+    uint64_t probe_stride = 0;
+    uint32_t chunks_per_q = 0;
+    uint32_t* heavy = nullptr;
+    uint32_t* lpref = nullptr;
+    uint64_t* lcnt = nullptr;
+    uint64_t* lpref_q = nullptr;
+    uint32_t* probe_list = nullptr;
+    uint32_t* n_probe = nullptr;
+    uint32_t* probe_bm = nullptr;
+    uint32_t* counts = nullptr;
+    uint64_t* offsets = nullptr;
+    uint64_t* scan_status = nullptr;
+    uint32_t* scan_counter = nullptr;
+    uint64_t* id_off = nullptr;
+    uint8_t* path_out = nullptr;
+    uint32_t* err = nullptr;
+    uint32_t* q_terms = nullptr;  // single-query staging (abf_query)
+    uint64_t* q_off = nullptr;
+};
+
+struct abf_worker {
+    abf_index* ix = nullptr;
+    int kind = 0;  // 0 sparse, 1 dense (host bitmaps copied), 2 dense (caller device bitmaps)
+    // sparse
+    uint64_t n_keys = 0;
+    uint32_t* d_keys = nullptr;
+    uint64_t* d_off1 = nullptr;     // {0, n_keys}: the keys as one query
+    uint64_t* d_offk = nullptr;     // 0..n_keys: every key its own query
+    uint32_t* d_heavy = nullptr;
+    uint32_t* d_lpref = nullptr;
+    uint64_t* d_lcnt = nullptr;
+    uint64_t* d_lpref_q = nullptr;
+    uint32_t* d_nprobe = nullptr;
+    // dense
+    uint64_t batch = 0;
+    uint64_t len = 0;               // bytes per query bitmap as given
+    uint32_t* d_qbm = nullptr;      // own copy, qbm_stride words per query
+    uint64_t qbm_stride = 0;
+    const uint8_t* d_ext = nullptr; // caller device bitmaps (kind 2)
+};
+
+namespace {
+
+template <class T>
+abf_status dev_alloc(T** p, uint64_t n, uint64_t* bytes = nullptr) {
+    uint64_t b = std::max<uint64_t>(n, 1) * sizeof(T);
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), b);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail(ABF_ERR_OOM, std::string("cudaMalloc(") + std::to_string(b) + "): " + cudaGetErrorString(e));
+    }
+    if (bytes) *bytes += b;
+    return ABF_OK;
+}
+
+template <class T>
+void dev_free(T*& p) {
+    if (p) cudaFree(const_cast<void*>(reinterpret_cast<const void*>(p)));
+    p = nullptr;
+}
+
+template <class T>
+abf_status upload_vec(T** dst, const std::vector<T>& v, uint64_t* bytes) {
+    ABF_TRY(dev_alloc(dst, v.size(), bytes));
+    if (!v.empty()) CUDA_TRY(cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return ABF_OK;
+}
+
+template <class T>
+abf_status download_vec(std::vector<T>& v, const T* src, uint64_t n) {
+    v.resize(n);
+    if (n) CUDA_TRY(cudaMemcpy(v.data(), src, n * sizeof(T), cudaMemcpyDeviceToHost));
+    return ABF_OK;
+}
+
+uint64_t n_words_of(uint64_t n_bits) { return (n_bits + 31) / 32; }
+uint64_t round4(uint64_t x) { return (x + 3) & ~uint64_t(3); }
+
+void default_tuning(abf_index* ix) {
+    abf_tuning& t = ix->tuning;
+    t.tile_words = 1024;
+    t.warps_per_tile = 8;
+    // a list is merged per tile when its blocks are on average no wider than
+    // one tile (128 ids per block spread over n_ads / len ids)
+    uint64_t span = uint64_t(t.tile_words) * 32u;
+    uint64_t m = (uint64_t(abf::kBlock) * ix->n_ads + span - 1) / span;
+    t.heavy_min_len = uint32_t(std::max<uint64_t>(m, abf::kBlock));
+    t.probe_chunk_blocks = 256;
+    t.scatter_blocks_per_warp = 4;
+    t.ctas_per_sm = 2;
+    t.probe_cap = 32;
+    t.probe_min_fraction = 0.5f;
+}
+
+void free_device(abf_index* ix) {
+    auto& d = ix->dev;
+    dev_free(d.term_blk);
+    dev_free(d.term_len);
+    dev_free(d.blk_first);
+    dev_free(d.blk_last);
+    dev_free(d.blk_term);
+    dev_free(d.blk_desc);
+    dev_free(d.payload);
+    d.bytes = 0;
+    ix->on_device = false;
+}
+
+abf_status upload(abf_index* ix, int device) {
+    CUDA_TRY(cudaSetDevice(device));
+    int sms = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    ix->sm_count = sms > 0 ? sms : 148;
+    ix->device = device;
+    auto& h = ix->host;
+    auto& d = ix->dev;
+    d.bytes = 0;
+    abf_status st = ABF_OK;
+    if ((st = upload_vec(&d.term_blk, h.term_blk, &d.bytes)) != ABF_OK ||
+        (st = upload_vec(&d.term_len, h.term_len, &d.bytes)) != ABF_OK ||
+        (st = upload_vec(&d.blk_first, h.blk_first, &d.bytes)) != ABF_OK ||
+        (st = upload_vec(&d.blk_last, h.blk_last, &d.bytes)) != ABF_OK ||
+        (st = upload_vec(&d.blk_term, h.blk_term, &d.bytes)) != ABF_OK ||
+        (st = upload_vec(&d.blk_desc, h.blk_desc, &d.bytes)) != ABF_OK ||
+        (st = upload_vec(&d.payload, h.payload, &d.bytes)) != ABF_OK) {
+        free_device(ix);
+        return st;
+    }
+    ix->on_device = true;
+    return ABF_OK;
+}
+
+abf_status finalize(abf_index* ix, const abf_build_opts* opts) {
+    auto& h = ix->host;
+    ix->n_terms = h.n_terms;
+    ix->n_ads = h.n_ads;
+    ix->n_postings = h.n_postings;
+    ix->max_list_len = h.max_list_len;
+    ix->n_blocks = h.n_blocks();
+    ix->payload_units = h.payload.size();
+    ix->h_term_blk = h.term_blk;
+    ix->h_term_len = h.term_len;
+    ix->h_term_bytes.assign(h.n_terms, 0);
+    for (uint32_t t = 0; t < h.n_terms; ++t) {
+        uint64_t bytes = 0;
+        for (uint32_t b = h.term_blk[t]; b < h.term_blk[t + 1]; ++b) {
+            const uint32_t meta = h.blk_desc[b].y;
+            bytes += 16u + 16ull * abf::payload_units(abf::desc_count(meta), abf::desc_bits(meta));
+        }
+        ix->h_term_bytes[t] = bytes;
+    }
+    ix->host_valid = true;
+    default_tuning(ix);
+    uint32_t flags = opts ? opts->flags : 0u;
+    if (!(flags & ABF_BUILD_HOST_ONLY)) {
+        ABF_TRY(upload(ix, opts ? opts->device : 0));
+        if (!(flags & ABF_BUILD_KEEP_HOST)) {
+            ix->host = abf::HostIndex();
+            ix->host_valid = false;
+        }
+    }
+    return ABF_OK;
+}
+
+abf_status need_device(const abf_index* ix) {
+    if (!ix) return fail(ABF_ERR_INVALID, "null index");
+    if (!ix->on_device) return fail(ABF_ERR_STATE, "index has no device copy (built with ABF_BUILD_HOST_ONLY)");
+    return ABF_OK;
+}
+
+void ws_release(abf_workspace* w) {
+    dev_free(w->heavy);
+    dev_free(w->lpref);
+    dev_free(w->lcnt);
+    dev_free(w->lpref_q);
+    dev_free(w->probe_list);
+    dev_free(w->n_probe);
+    dev_free(w->probe_bm);
+    dev_free(w->counts);
+    dev_free(w->offsets);
+    dev_free(w->scan_status);
+    dev_free(w->scan_counter);
+    dev_free(w->id_off);
+    dev_free(w->path_out);
+    dev_free(w->err);
+    dev_free(w->q_terms);
+    dev_free(w->q_off);
+}
+
+abf_status ws_alloc(abf_index* ix, uint32_t max_q, uint64_t max_terms, uint64_t max_bits, abf_workspace* w) {
+    w->ix = ix;
+    w->max_q = max_q;
+    w->max_terms = max_terms;
+    w->probe_cap = ix->tuning.probe_cap;
+    w->probe_stride = round4(n_words_of(ix->n_terms));
+    w->chunks_per_q = abf::compact_chunks(std::max<uint64_t>(max_bits, ix->n_ads));
+    const uint64_t chunks = uint64_t(max_q) * w->chunks_per_q;
+    abf_status st;
+    if ((st = dev_alloc(&w->heavy, max_q)) != ABF_OK || (st = dev_alloc(&w->lpref, max_terms)) != ABF_OK ||
+        (st = dev_alloc(&w->lcnt, max_q)) != ABF_OK || (st = dev_alloc(&w->lpref_q, uint64_t(max_q) + 1)) != ABF_OK ||
+        (st = dev_alloc(&w->probe_list, w->probe_cap)) != ABF_OK || (st = dev_alloc(&w->n_probe, 1)) != ABF_OK ||
+        (st = dev_alloc(&w->probe_bm, uint64_t(w->probe_cap) * w->probe_stride)) != ABF_OK ||
+        (st = dev_alloc(&w->counts, chunks)) != ABF_OK || (st = dev_alloc(&w->offsets, chunks + 1)) != ABF_OK ||
+        (st = dev_alloc(&w->scan_status, abf::scan_tiles(chunks))) != ABF_OK ||
+        (st = dev_alloc(&w->scan_counter, 1)) != ABF_OK || (st = dev_alloc(&w->id_off, uint64_t(max_q) + 1)) != ABF_OK ||
+        (st = dev_alloc(&w->path_out, max_q)) != ABF_OK || (st = dev_alloc(&w->err, 1)) != ABF_OK ||
+        (st = dev_alloc(&w->q_terms, max_terms)) != ABF_OK || (st = dev_alloc(&w->q_off, 2)) != ABF_OK) {
+        ws_release(w);
+        return st;
+    }
+    CUDA_TRY(cudaMemset(w->err, 0, sizeof(uint32_t)));
+    return ABF_OK;
+}
+
+// the index's own workspace, grown to fit (growth synchronises the device)
+abf_status own_ws(abf_index* ix, uint32_t n_q, uint64_t n_terms, uint64_t n_bits, abf_workspace** out) {
+    abf_workspace* w = ix->own_ws;
+    uint32_t need_chunks = abf::compact_chunks(std::max<uint64_t>(n_bits, ix->n_ads));
+    if (w && w->max_q >= n_q && w->max_terms >= n_terms && w->chunks_per_q >= need_chunks &&
+        w->probe_cap == ix->tuning.probe_cap) {
+        *out = w;
+        return ABF_OK;
+    }
+    uint32_t mq = std::max<uint32_t>(n_q, w ? w->max_q : 1u);
+    uint64_t mt = std::max<uint64_t>({n_terms, w ? w->max_terms : 0ull, 4096ull});
+    uint64_t mb = std::max<uint64_t>(n_bits, ix->n_ads);
+    if (w) {
+        CUDA_TRY(cudaDeviceSynchronize());
+        ws_release(w);
+    } else {
+        w = new abf_workspace();
+    }
+    abf_status st = ws_alloc(ix, mq, mt, mb, w);
+    if (st != ABF_OK) {
+        delete w;
+        ix->own_ws = nullptr;
+        return st;
+    }
+    ix->own_ws = w;
+    *out = w;
+    return ABF_OK;
+}
+
+struct RunOpts {
+    uint64_t* id_counts = nullptr;
+};
+
+abf_status run_compact(abf_index* ix, const abf::CompactArgs& ca, cudaStream_t s) {
+    TIMED(K_COUNT, abf::launch_compact_count(ca, ix->sm_count, s));
+    TIMED(K_SCAN, abf::launch_compact_scan(ca, s));
+    TIMED(K_WRITE, abf::launch_compact_write(ca, ix->sm_count, s));
+    return ABF_OK;
+}
+
+abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const RunOpts& ro, cudaStream_t s) {
+    if (b->n_queries == 0) return ABF_OK;
+    if (b->n_queries > ws->max_q) return fail(ABF_ERR_CAPACITY, "batch has more queries than the workspace");
+    const uint64_t n_words = n_words_of(ix->n_ads);
+    if (b->bitmap_stride_words < n_words) return fail(ABF_ERR_INVALID, "bitmap_stride_words < (n_ads+31)/32");
+    if (b->d_ids && !b->d_id_offsets && !ro.id_counts)
+        return fail(ABF_ERR_INVALID, "d_ids needs d_id_offsets");
+    CUDA_TRY(cudaSetDevice(ix->device));
+    const abf::IndexView v = abf::view_of(ix);
+    const abf_tuning& t = ix->tuning;
+    CUDA_TRY(cudaMemsetAsync(ws->n_probe, 0, sizeof(uint32_t), s));
+    abf::PlanArgs pa{};
+    pa.terms = b->d_terms;
+    pa.q_off = b->d_offsets;
+    pa.n_q = b->n_queries;
+    pa.paths = b->d_paths;
+    pa.path_uniform = uint32_t(b->path);
+    pa.hybrid_min = t.heavy_min_len;
+    pa.probe_min_frac = t.probe_min_fraction;
+    pa.heavy_min = ws->heavy;
+    pa.term_lpref = ws->lpref;
+    pa.q_light_cnt = ws->lcnt;
+    pa.probe_list = ws->probe_list;
+    pa.n_probe = ws->n_probe;
+    pa.probe_cap = ws->probe_cap;
+    pa.path_out = ws->path_out;
+    pa.max_terms = ws->max_terms;
+    pa.err = ws->err;
+    TIMED(K_PLAN, abf::launch_plan(v, pa, s));
+    abf::QueueArgs qa{ws->lcnt, ws->lpref_q, b->n_queries};
+    TIMED(K_QUEUE, abf::launch_queue_scan(qa, s));
+    const bool maybe_probe = ws->probe_cap > 0 && (b->d_paths || b->path == ABF_PATH_PROBE || b->path == ABF_PATH_AUTO);
+    if (maybe_probe) {
+        CUDA_TRY(cudaMemsetAsync(ws->probe_bm, 0, uint64_t(ws->probe_cap) * ws->probe_stride * 4u, s));
+        abf::ProbeBitsArgs pb{b->d_terms, b->d_offsets, ws->probe_list, ws->n_probe, ws->probe_bm, ws->probe_stride,
+                              ix->n_terms};
+        TIMED(K_PROBE_BITS, abf::launch_probe_bits(pb, ws->probe_cap, s));
+    }
+    abf::TileArgs ta{};
+    ta.terms = b->d_terms;
+    ta.q_off = b->d_offsets;
+    ta.heavy_min = ws->heavy;
+    ta.n_q = b->n_queries;
+    ta.n_tiles = uint32_t((n_words + t.tile_words - 1) / t.tile_words);
+    ta.out = b->d_bitmaps;
+    ta.out_stride = b->bitmap_stride_words;
+    ta.n_words = n_words;
+    ta.accumulate = 0;
+    TIMED(K_TILE, abf::launch_tile_union(v, ta, t, ix->sm_count, s));
+    abf::ScatterArgs sa{};
+    sa.terms = b->d_terms;
+    sa.q_off = b->d_offsets;
+    sa.term_lpref = ws->lpref;
+    sa.q_light_pref = ws->lpref_q;
+    sa.n_q = b->n_queries;
+    sa.out = b->d_bitmaps;
+    sa.out_stride = b->bitmap_stride_words;
+    sa.blocks_per_warp = std::max<uint32_t>(1u, t.scatter_blocks_per_warp);
+    TIMED(K_SCATTER, abf::launch_scatter(v, sa, t, ix->sm_count, s));
+    if (maybe_probe) {
+        abf::ProbeArgs pr{};
+        pr.qbm = ws->probe_bm;
+        pr.qbm_stride = ws->probe_stride;
+        pr.qbm_words = uint32_t(ws->probe_stride);
+        pr.staged_ok = 1;
+        pr.d_n_probe = ws->n_probe;
+        pr.out_slot = ws->probe_list;
+        pr.out = b->d_bitmaps;
+        pr.out_stride = b->bitmap_stride_words;
+        pr.chunk_blocks = t.probe_chunk_blocks;
+        pr.err = ws->err;
+        TIMED(K_PROBE, abf::launch_probe(v, pr, t, ix->sm_count, s));
+    }
+    if (b->d_ids || ro.id_counts) {
+        abf::CompactArgs ca{};
+        ca.bm = b->d_bitmaps;
+        ca.stride = b->bitmap_stride_words;
+        ca.n_q = b->n_queries;
+        ca.n_bits = ix->n_ads;
+        ca.n_chunks = abf::compact_chunks(ix->n_ads);
+        ca.counts = ws->counts;
+        ca.offsets = ws->offsets;
+        ca.scan_status = ws->scan_status;
+        ca.scan_counter = ws->scan_counter;
+        ca.ids = b->d_ids;
+        ca.capacity = b->d_ids ? b->ids_capacity : 0;
+        ca.id_offsets = b->d_id_offsets ? b->d_id_offsets : ws->id_off;
+        ca.id_counts = ro.id_counts;
+        ca.err = ws->err;
+        ABF_TRY(run_compact(ix, ca, s));
+    }
+    return ABF_OK;
+}
+
+abf_status worker_plan_scratch(abf_worker* w, uint64_t n_q) {
+    ABF_TRY(dev_alloc(&w->d_heavy, n_q));
+    ABF_TRY(dev_alloc(&w->d_lpref, std::max<uint64_t>(w->n_keys, 1)));
+    ABF_TRY(dev_alloc(&w->d_lcnt, n_q));
+    ABF_TRY(dev_alloc(&w->d_lpref_q, n_q + 1));
+    ABF_TRY(dev_alloc(&w->d_nprobe, 1));
+    return ABF_OK;
+}
+
+void worker_release(abf_worker* w) {
+    dev_free(w->d_keys);
+    dev_free(w->d_off1);
+    dev_free(w->d_offk);
+    dev_free(w->d_heavy);
+    dev_free(w->d_lpref);
+    dev_free(w->d_lcnt);
+    dev_free(w->d_lpref_q);
+    dev_free(w->d_nprobe);
+    dev_free(w->d_qbm);
+}
+
+// plan + scatter (and, for one query, merge tiles) of a sparse worker
+abf_status run_sparse(const abf_worker* w, uint32_t* d_res, bool keyed, const uint32_t* d_qidx,
+                      uint64_t res_stride_words, cudaStream_t s) {
+    abf_index* ix = w->ix;
+    ABF_TRY(need_device(ix));
+    if (!d_res) return fail(ABF_ERR_INVALID, "null d_res");
+    if (w->n_keys == 0) return ABF_OK;
+    CUDA_TRY(cudaSetDevice(ix->device));
+    const abf::IndexView v = abf::view_of(ix);
+    const abf_tuning& t = ix->tuning;
+    const uint32_t n_q = keyed ? uint32_t(w->n_keys) : 1u;
+    const uint64_t* q_off = keyed ? w->d_offk : w->d_off1;
+    abf::PlanArgs pa{};
+    pa.terms = w->d_keys;
+    pa.q_off = q_off;
+    pa.n_q = n_q;
+    // keyed batches may map several keys to one bitmap: only atomic
+    // scatters are safe there; a single query merges its long lists per tile
+    pa.path_uniform = keyed ? ABF_PATH_UNION : ABF_PATH_HYBRID;
+    pa.hybrid_min = t.heavy_min_len;
+    pa.heavy_min = w->d_heavy;
+    pa.term_lpref = w->d_lpref;
+    pa.q_light_cnt = w->d_lcnt;
+    pa.n_probe = w->d_nprobe;
+    pa.probe_cap = 0;
+    pa.max_terms = w->n_keys;
+    pa.err = nullptr;
+    CUDA_TRY(cudaMemsetAsync(w->d_nprobe, 0, sizeof(uint32_t), s));
+    TIMED(K_PLAN, abf::launch_plan(v, pa, s));
+    abf::QueueArgs qa{w->d_lcnt, w->d_lpref_q, n_q};
+    TIMED(K_QUEUE, abf::launch_queue_scan(qa, s));
+    const uint64_t n_words = n_words_of(ix->n_ads);
+    if (!keyed) {
+        abf::TileArgs ta{};
+        ta.terms = w->d_keys;
+        ta.q_off = q_off;
+        ta.heavy_min = w->d_heavy;
+        ta.n_q = 1;
+        ta.n_tiles = uint32_t((n_words + t.tile_words - 1) / t.tile_words);
+        ta.out = d_res;
+        ta.out_stride = n_words;
+        ta.n_words = n_words;
+        ta.accumulate = 1;
+        TIMED(K_TILE, abf::launch_tile_union(v, ta, t, ix->sm_count, s));
+    }
+    abf::ScatterArgs sa{};
+    sa.terms = w->d_keys;
+    sa.q_off = q_off;
+    sa.term_lpref = w->d_lpref;
+    sa.q_light_pref = w->d_lpref_q;
+    sa.n_q = n_q;
+    sa.out_slot = keyed ? d_qidx : nullptr;
+    sa.out = d_res;
+    sa.out_stride = res_stride_words;
+    sa.blocks_per_warp = std::max<uint32_t>(1u, t.scatter_blocks_per_warp);
+    TIMED(K_SCATTER, abf::launch_scatter(v, sa, t, ix->sm_count, s));
+    return ABF_OK;
+}
+
+abf_status run_dense(const abf_worker* w, uint32_t* d_res, uint64_t res_stride_words, cudaStream_t s) {
+    abf_index* ix = w->ix;
+    ABF_TRY(need_device(ix));
+    if (!d_res) return fail(ABF_ERR_INVALID, "null d_res");
+    if (w->batch == 0) return ABF_OK;
+    CUDA_TRY(cudaSetDevice(ix->device));
+    abf::ProbeArgs pr{};
+    if (w->kind == 2) {
+        pr.qbm = reinterpret_cast<const uint32_t*>(w->d_ext);
+        pr.qbm_stride = w->len / 4;
+        pr.qbm_words = uint32_t(std::min<uint64_t>(w->len / 4, 0xffffffffull));
+        pr.staged_ok = (reinterpret_cast<uintptr_t>(w->d_ext) % 16 == 0) && ((w->len / 4) % 4 == 0);
+    } else {
+        pr.qbm = w->d_qbm;
+        pr.qbm_stride = w->qbm_stride;
+        pr.qbm_words = uint32_t(w->qbm_stride);
+        pr.staged_ok = 1;
+    }
+    pr.d_n_probe = nullptr;
+    pr.n_probe_host = uint32_t(w->batch);
+    pr.out_slot = nullptr;
+    pr.out = d_res;
+    pr.out_stride = res_stride_words;
+    pr.chunk_blocks = ix->tuning.probe_chunk_blocks;
+    abf_workspace* ws = nullptr;
+    ABF_TRY(own_ws(ix, 1, 1, ix->n_ads, &ws));
+    pr.err = ws->err;
+    TIMED(K_PROBE, abf::launch_probe(abf::view_of(ix), pr, ix->tuning, ix->sm_count, s));
+    return ABF_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// exported API
+// ===========================================================================
+extern "C" {
+
+const char* abf_last_error_string(void) { return g_err.c_str(); }
+
+const char* abf_status_string(abf_status s) {
+    switch (s) {
+        case ABF_OK: return "ok";
+        case ABF_ERR_INVALID: return "invalid argument";
+        case ABF_ERR_RANGE: return "id out of range";
+        case ABF_ERR_CUDA: return "CUDA error";
+        case ABF_ERR_OOM: return "out of memory";
+        case ABF_ERR_STATE: return "invalid state";
+        case ABF_ERR_IO: return "I/O error";
+        case ABF_ERR_TIMEOUT: return "device wait timed out";
+        case ABF_ERR_CAPACITY: return "capacity exceeded";
+        default: return "internal error";
+    }
+}
+
+uint32_t abf_abi_version(void) { return ABF_ABI_VERSION; }
+uint64_t abf_launch_count(void) { return g_launches.load(); }
+
+abf_status abf_index_build_csr(const uint64_t* offsets, const uint32_t* ads, uint32_t n_terms, uint32_t n_ads,
+                               const abf_build_opts* opts, abf_index** out) {
+    API_BEGIN
+    abf::clear_error();
+    if (!offsets || !out || n_terms == 0 || n_ads == 0) return fail(ABF_ERR_INVALID, "abf_index_build_csr: bad arguments");
+    if (n_ads > (1u << 31)) return fail(ABF_ERR_RANGE, "n_ads above 2^31");
+    if (offsets[0] != 0) return fail(ABF_ERR_INVALID, "offsets[0] must be 0");
+    for (uint32_t t = 0; t < n_terms; ++t)
+        if (offsets[t + 1] < offsets[t]) return fail(ABF_ERR_INVALID, "offsets not monotone");
+    if (offsets[n_terms] && !ads) return fail(ABF_ERR_INVALID, "null ads");
+    *out = nullptr;
+    abf_index* ix = new abf_index();
+    abf_status st = abf::build_host(offsets, ads, n_terms, n_ads, opts ? opts->n_threads : 0, &ix->host);
+    if (st == ABF_OK) st = finalize(ix, opts);
+    if (st != ABF_OK) {
+        free_device(ix);
+        delete ix;
+        return st;
+    }
+    *out = ix;
+    return ABF_OK;
+    API_END
+}
+
+abf_status abf_index_build_coo(const uint32_t* terms, const uint32_t* ads, uint64_t nnz, uint32_t n_terms,
+                               uint32_t n_ads, const abf_build_opts* opts, abf_index** out) {
+    API_BEGIN
+    abf::clear_error();
+    if (!out || n_terms == 0 || n_ads == 0 || (nnz && (!terms || !ads)))
+        return fail(ABF_ERR_INVALID, "abf_index_build_coo: bad arguments");
+    std::vector<uint64_t> off;
+    std::vector<uint32_t> csr;
+    ABF_TRY(abf::coo_to_csr(terms, ads, nnz, n_terms, n_ads, opts ? opts->n_threads : 0, &off, &csr));
+    return abf_index_build_csr(off.data(), csr.data(), n_terms, n_ads, opts, out);
+    API_END
+}
+
+abf_status abf_index_free(abf_index* ix) {
+    API_BEGIN
+    if (!ix) return ABF_OK;
+    if (ix->on_device) {
+        cudaSetDevice(ix->device);
+        cudaDeviceSynchronize();
+    }
+    if (ix->own_ws) {
+        ws_release(ix->own_ws);
+        delete ix->own_ws;
+    }
+    if (ix->h_stage) cudaFreeHost(ix->h_stage);
+    if (ix->stage_event) cudaEventDestroy(static_cast<cudaEvent_t>(ix->stage_event));
+    delete static_cast<Profiler*>(ix->prof);
+    ix->prof = nullptr;
+    free_device(ix);
+    delete ix;
+    return ABF_OK;
+    API_END
+}
+
+abf_status abf_index_get_stats(const abf_index* ix, abf_index_stats* o) {
+    if (!ix || !o) return fail(ABF_ERR_INVALID, "null argument");
+    o->n_terms = ix->n_terms;
+    o->n_ads = ix->n_ads;
+    o->n_postings = ix->n_postings;
+    o->n_blocks = ix->n_blocks;
+    o->payload_bytes = (ix->payload_units ? ix->payload_units - 1 : 0) * 16ull;
+    o->device_bytes = ix->dev.bytes;
+    o->max_list_len = ix->max_list_len;
+    o->on_device = ix->on_device ? 1u : 0u;
+    return ABF_OK;
+}
+
+abf_status abf_index_list_lengths(const abf_index* ix, uint32_t* h_out, uint32_t n) {
+    if (!ix || !h_out || n < ix->n_terms) return fail(ABF_ERR_INVALID, "abf_index_list_lengths: bad arguments");
+    std::memcpy(h_out, ix->h_term_len.data(), size_t(ix->n_terms) * 4);
+    return ABF_OK;
+}
+
+abf_status abf_index_decode_list(const abf_index* ix, uint32_t term, uint32_t* h_ids, uint64_t cap, uint64_t* n_out) {
+    API_BEGIN
+    if (!ix || !n_out) return fail(ABF_ERR_INVALID, "null argument");
+    if (!ix->host_valid) return fail(ABF_ERR_STATE, "no host copy (build with ABF_BUILD_KEEP_HOST or HOST_ONLY)");
+    if (term >= ix->n_terms) return fail(ABF_ERR_RANGE, "term >= n_terms");
+    const auto& h = ix->host;
+    *n_out = h.term_len[term];
+    uint32_t buf[abf::kBlock];
+    uint64_t k = 0;
+    for (uint32_t b = h.term_blk[term]; b < h.term_blk[term + 1]; ++b) {
+        abf::decode_block_host(h, b, buf);
+        uint32_t cnt = abf::desc_count(h.blk_desc[b].y);
+        for (uint32_t i = 0; i < cnt; ++i, ++k)
+            if (h_ids && k < cap) h_ids[k] = buf[i];
+    }
+    return ABF_OK;
+    API_END
+}
+
+abf_status abf_index_save(const abf_index* ix, const char* path) {
+    API_BEGIN
+    if (!ix || !path) return fail(ABF_ERR_INVALID, "null argument");
+    if (ix->host_valid) return abf::save_host(ix->host, path);
+    abf::HostIndex h;
+    h.n_terms = ix->n_terms;
+    h.n_ads = ix->n_ads;
+    h.n_postings = ix->n_postings;
+    h.max_list_len = ix->max_list_len;
+    CUDA_TRY(cudaSetDevice(ix->device));
+    ABF_TRY(download_vec(h.term_blk, ix->dev.term_blk, uint64_t(ix->n_terms) + 1));
+    ABF_TRY(download_vec(h.term_len, ix->dev.term_len, ix->n_terms));
+    ABF_TRY(download_vec(h.blk_first, ix->dev.blk_first, ix->n_blocks));
+    ABF_TRY(download_vec(h.blk_last, ix->dev.blk_last, ix->n_blocks));
+    ABF_TRY(download_vec(h.blk_term, ix->dev.blk_term, ix->n_blocks));
+    ABF_TRY(download_vec(h.blk_desc, ix->dev.blk_desc, ix->n_blocks));
+    ABF_TRY(download_vec(h.payload, ix->dev.payload, ix->payload_units));
+    return abf::save_host(h, path);
+    API_END
+}
+
+abf_status abf_index_load(const char* path, const abf_build_opts* opts, abf_index** out) {
+    API_BEGIN
+    abf::clear_error();
+    if (!path || !out) return fail(ABF_ERR_INVALID, "null argument");
+    *out = nullptr;
+    abf_index* ix = new abf_index();
+    abf_status st = abf::load_host(path, &ix->host);
+    if (st == ABF_OK) st = finalize(ix, opts);
+    if (st != ABF_OK) {
+        free_device(ix);
+        delete ix;
+        return st;
+    }
+    *out = ix;
+    return ABF_OK;
+    API_END
+}
+
+abf_status abf_index_to_device(abf_index* ix, int device) {
+    API_BEGIN
+    if (!ix) return fail(ABF_ERR_INVALID, "null index");
+    if (ix->on_device) return ABF_OK;
+    if (!ix->host_valid) return fail(ABF_ERR_STATE, "no host copy to upload");
+    return upload(ix, device);
+    API_END
+}
+
+abf_status abf_get_tuning(const abf_index* ix, abf_tuning* out) {
+    if (!ix || !out) return fail(ABF_ERR_INVALID, "null argument");
+    *out = ix->tuning;
+    return ABF_OK;
+}
+
+abf_status abf_set_tuning(abf_index* ix, const abf_tuning* t) {
+    if (!ix || !t) return fail(ABF_ERR_INVALID, "null argument");
+    if (t->tile_words != 256 && t->tile_words != 512 && t->tile_words != 1024)
+        return fail(ABF_ERR_INVALID, "tile_words must be 256, 512 or 1024");
+    if (t->warps_per_tile != 1 && t->warps_per_tile != 2 && t->warps_per_tile != 4 && t->warps_per_tile != 8)
+        return fail(ABF_ERR_INVALID, "warps_per_tile must be 1, 2, 4 or 8");
+    if (t->probe_chunk_blocks == 0 || t->probe_chunk_blocks % 128 != 0)
+        return fail(ABF_ERR_INVALID, "probe_chunk_blocks must be a positive multiple of 128");
+    if (t->scatter_blocks_per_warp == 0 || t->ctas_per_sm == 0 || t->ctas_per_sm > 32)
+        return fail(ABF_ERR_INVALID, "scatter_blocks_per_warp and ctas_per_sm (<= 32) must be positive");
+    if (t->probe_cap > 4096) return fail(ABF_ERR_INVALID, "probe_cap above 4096");
+    ix->tuning = *t;
+    return ABF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// reference-shaped workers
+// ---------------------------------------------------------------------------
+abf_status abf_prepare_sparse(abf_index* ix, const uint32_t* keys, uint64_t n_keys, abf_worker** out) {
+    API_BEGIN
+    ABF_TRY(need_device(ix));
+    if (!out || (n_keys && !keys)) return fail(ABF_ERR_INVALID, "abf_prepare_sparse: bad arguments");
+    if (n_keys >= (1ull << 32)) return fail(ABF_ERR_RANGE, "too many keys");
+    CUDA_TRY(cudaSetDevice(ix->device));
+    *out = nullptr;
+    abf_worker* w = new abf_worker();
+    w->ix = ix;
+    w->kind = 0;
+    w->n_keys = n_keys;
+    std::vector<uint64_t> offk(n_keys + 1);
+    for (uint64_t i = 0; i <= n_keys; ++i) offk[i] = i;
+    uint64_t off1[2] = {0, n_keys};
+    abf_status st = ABF_OK;
+    if ((st = dev_alloc(&w->d_keys, n_keys)) != ABF_OK || (st = dev_alloc(&w->d_off1, 2)) != ABF_OK ||
+        (st = dev_alloc(&w->d_offk, n_keys + 1)) != ABF_OK ||
+        (st = worker_plan_scratch(w, std::max<uint64_t>(n_keys, 1))) != ABF_OK) {
+        worker_release(w);
+        delete w;
+        return st;
+    }
+    cudaError_t e = cudaSuccess;
+    if (n_keys) e = cudaMemcpy(w->d_keys, keys, n_keys * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(w->d_off1, off1, sizeof(off1), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(w->d_offk, offk.data(), offk.size() * 8, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        worker_release(w);
+        delete w;
+        return fail(ABF_ERR_CUDA, std::string("abf_prepare_sparse upload: ") + cudaGetErrorString(e));
+    }
+    *out = w;
+    return ABF_OK;
+    API_END
+}
+
+static abf_status prepare_dense_impl(abf_index* ix, uint64_t batch, uint64_t len, const uint8_t* bm, bool device,
+                                     abf_worker** out) {
+    ABF_TRY(need_device(ix));
+    if (!out || (batch && !bm)) return fail(ABF_ERR_INVALID, "dense prepare: bad arguments");
+    if (batch > 1 && len % 4 != 0) return fail(ABF_ERR_INVALID, "batch bitmap length must be a multiple of 4 bytes");
+    CUDA_TRY(cudaSetDevice(ix->device));
+    *out = nullptr;
+    abf_worker* w = new abf_worker();
+    w->ix = ix;
+    w->batch = batch;
+    w->len = len;
+    if (device) {
+        w->kind = 2;
+        w->d_ext = bm;
+        *out = w;
+        return ABF_OK;
+    }
+    w->kind = 1;
+    // own copy, padded so every query covers all n_terms bits and starts
+    // 16-byte aligned (bulk copies into shared memory need both)
+    w->qbm_stride = round4(std::max<uint64_t>(n_words_of(ix->n_terms), 1));
+    abf_status st = dev_alloc(&w->d_qbm, std::max<uint64_t>(batch, 1) * w->qbm_stride);
+    if (st != ABF_OK) {
+        delete w;
+        return st;
+    }
+    const uint64_t copy = std::min<uint64_t>(len, w->qbm_stride * 4);
+    cudaError_t e = cudaMemset(w->d_qbm, 0, std::max<uint64_t>(batch, 1) * w->qbm_stride * 4);
+    if (e == cudaSuccess && batch && copy)
+        e = cudaMemcpy2D(w->d_qbm, w->qbm_stride * 4, bm, len, copy, batch, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        worker_release(w);
+        delete w;
+        return fail(ABF_ERR_CUDA, std::string("dense prepare upload: ") + cudaGetErrorString(e));
+    }
+    *out = w;
+    return ABF_OK;
+}
+
+abf_status abf_prepare_dense(abf_index* ix, uint64_t len, const uint8_t* bm, abf_worker** out) {
+    API_BEGIN
+    return prepare_dense_impl(ix, 1, len, bm, false, out);
+    API_END
+}
+
+abf_status abf_prepare_batch(abf_index* ix, uint64_t batch, uint64_t len, const uint8_t* bm, abf_worker** out) {
+    API_BEGIN
+    return prepare_dense_impl(ix, batch, len, bm, false, out);
+    API_END
+}
+
+abf_status abf_prepare_batch_device(abf_index* ix, uint64_t batch, uint64_t len, const uint8_t* d_bm,
+                                    abf_worker** out) {
+    API_BEGIN
+    return prepare_dense_impl(ix, batch, len, d_bm, true, out);
+    API_END
+}
+
+abf_status abf_worker_free(abf_worker* w) {
+    API_BEGIN
+    if (!w) return ABF_OK;
+    if (w->ix && w->ix->on_device) {
+        cudaSetDevice(w->ix->device);
+        cudaDeviceSynchronize();
+    }
+    worker_release(w);
+    delete w;
+    return ABF_OK;
+    API_END
+}
+
+abf_status abf_list_union_sparse(const abf_worker* w, uint32_t* d_res, void* stream) {
+    API_BEGIN
+    if (!w || w->kind != 0) return fail(ABF_ERR_INVALID, "abf_list_union_sparse needs a sparse worker");
+    return run_sparse(w, d_res, false, nullptr, n_words_of(w->ix->n_ads), static_cast<cudaStream_t>(stream));
+    API_END
+}
+
+abf_status abf_batch_list_union_sparse(const abf_worker* w, uint32_t* d_res, const uint32_t* d_qidx,
+                                       uint32_t res_len_bytes, void* stream) {
+    API_BEGIN
+    if (!w || w->kind != 0) return fail(ABF_ERR_INVALID, "abf_batch_list_union_sparse needs a sparse worker");
+    if (!d_qidx && w->n_keys) return fail(ABF_ERR_INVALID, "null d_qidx");
+    if (uint64_t(res_len_bytes) * 8 < w->ix->n_ads) return fail(ABF_ERR_INVALID, "res_len_bytes smaller than the bitmap");
+    return run_sparse(w, d_res, true, d_qidx, res_len_bytes / 4, static_cast<cudaStream_t>(stream));
+    API_END
+}
+
+abf_status abf_list_union_dense(const abf_worker* w, uint32_t* d_res, void* stream) {
+    API_BEGIN
+    if (!w || w->kind == 0 || w->batch != 1) return fail(ABF_ERR_INVALID, "abf_list_union_dense needs a dense worker of one query");
+    return run_dense(w, d_res, n_words_of(w->ix->n_ads), static_cast<cudaStream_t>(stream));
+    API_END
+}
+
+abf_status abf_batch_list_union_dense(const abf_worker* w, uint32_t* d_res, uint32_t res_len_u32, void* stream) {
+    API_BEGIN
+    if (!w || w->kind == 0) return fail(ABF_ERR_INVALID, "abf_batch_list_union_dense needs a dense worker");
+    if (w->batch > 1 && uint64_t(res_len_u32) * 32 < w->ix->n_ads)
+        return fail(ABF_ERR_INVALID, "res_len_u32 smaller than the bitmap");
+    return run_dense(w, d_res, res_len_u32, static_cast<cudaStream_t>(stream));
+    API_END
+}
+
+abf_status abf_collect_ids(abf_index* ix, const uint32_t* d_bitmap, uint64_t n_bits, uint32_t* d_ids,
+                           uint64_t ids_capacity, uint64_t* d_count, void* stream) {
+    API_BEGIN
+    ABF_TRY(need_device(ix));
+    if (!d_bitmap || !d_count || (ids_capacity && !d_ids)) return fail(ABF_ERR_INVALID, "abf_collect_ids: bad arguments");
+    if (n_bits == 0 || n_bits > (1ull << 32)) return fail(ABF_ERR_RANGE, "n_bits must be in [1, 2^32]");
+    CUDA_TRY(cudaSetDevice(ix->device));
+    abf_workspace* ws = nullptr;
+    ABF_TRY(own_ws(ix, 1, 1, n_bits, &ws));
+    abf::CompactArgs ca{};
+    ca.bm = d_bitmap;
+    ca.stride = n_words_of(n_bits);
+    ca.n_q = 1;
+    ca.n_bits = n_bits;
+    ca.n_chunks = abf::compact_chunks(n_bits);
+    ca.counts = ws->counts;
+    ca.offsets = ws->offsets;
+    ca.scan_status = ws->scan_status;
+    ca.scan_counter = ws->scan_counter;
+    ca.ids = d_ids;
+    ca.capacity = ids_capacity;
+    ca.id_offsets = ws->id_off;
+    ca.id_counts = d_count;
+    ca.err = ws->err;
+    ABF_TRY(run_compact(ix, ca, static_cast<cudaStream_t>(stream)));
+    return ABF_OK;
+    API_END
+}
+
+// ---------------------------------------------------------------------------
+// native batch API
+// ---------------------------------------------------------------------------
+abf_status abf_workspace_create(abf_index* ix, uint32_t max_queries, uint64_t max_terms, abf_workspace** out) {
+    API_BEGIN
+    ABF_TRY(need_device(ix));
+    if (!out || max_queries == 0) return fail(ABF_ERR_INVALID, "abf_workspace_create: bad arguments");
+    CUDA_TRY(cudaSetDevice(ix->device));
+    *out = nullptr;
+    abf_workspace* w = new abf_workspace();
+    abf_status st = ws_alloc(ix, max_queries, std::max<uint64_t>(max_terms, 1), ix->n_ads, w);
+    if (st != ABF_OK) {
+        delete w;
+        return st;
+    }
+    *out = w;
+    return ABF_OK;
+    API_END
+}
+
+abf_status abf_workspace_free(abf_workspace* w) {
+    API_BEGIN
+    if (!w) return ABF_OK;
+    if (w->ix && w->ix->on_device) {
+        cudaSetDevice(w->ix->device);
+        cudaDeviceSynchronize();
+    }
+    ws_release(w);
+    delete w;
+    return ABF_OK;
+    API_END
+}
+
+abf_status abf_workspace_check(abf_workspace* w, void* stream) {
+    API_BEGIN
+    if (!w) return fail(ABF_ERR_INVALID, "null workspace");
+    CUDA_TRY(cudaSetDevice(w->ix->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    uint32_t err = 0;
+    CUDA_TRY(cudaMemcpyAsync(&err, w->err, 4, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    CUDA_TRY(cudaMemsetAsync(w->err, 0, 4, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    if (err & abf::kErrTermRange) return fail(ABF_ERR_CAPACITY, "a query's term offsets exceed the workspace's max_terms");
+    if (err) return fail(ABF_ERR_TIMEOUT, "a bounded device wait gave up (code " + std::to_string(err) + ")");
+    return ABF_OK;
+    API_END
+}
+
+abf_status abf_batch_run(abf_index* ix, abf_workspace* ws, const abf_batch* b, void* stream) {
+    API_BEGIN
+    ABF_TRY(need_device(ix));
+    if (!ws || !b || ws->ix != ix) return fail(ABF_ERR_INVALID, "abf_batch_run: bad arguments");
+    if (b->n_queries && (!b->d_terms || !b->d_offsets || !b->d_bitmaps))
+        return fail(ABF_ERR_INVALID, "abf_batch_run: null device array");
+    return run_batch(ix, ws, b, RunOpts{}, static_cast<cudaStream_t>(stream));
+    API_END
+}
+
+abf_status abf_query(abf_index* ix, const uint32_t* terms, uint32_t n_terms, abf_path path, uint32_t* d_bitmap,
+                     uint32_t* d_ids, uint64_t ids_capacity, uint64_t* d_count, void* stream) {
+    API_BEGIN
+    ABF_TRY(need_device(ix));
+    if (!d_bitmap || (n_terms && !terms) || (d_ids && !d_count))
+        return fail(ABF_ERR_INVALID, "abf_query: bad arguments");
+    CUDA_TRY(cudaSetDevice(ix->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    abf_workspace* ws = nullptr;
+    ABF_TRY(own_ws(ix, 1, n_terms, ix->n_ads, &ws));
+    const size_t need = size_t(n_terms) * 4 + 16;
+    if (!ix->stage_event) {
+        cudaEvent_t ev;
+        CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        ix->stage_event = ev;
+    }
+    cudaEvent_t ev = static_cast<cudaEvent_t>(ix->stage_event);
+    CUDA_TRY(cudaEventSynchronize(ev));  // the previous upload has left the staging buffer
+    if (ix->h_stage_bytes < need) {
+        if (ix->h_stage) cudaFreeHost(ix->h_stage);
+        ix->h_stage = nullptr;
+        ix->h_stage_bytes = 0;
+        CUDA_TRY(cudaMallocHost(&ix->h_stage, std::max<size_t>(need, 4096)));
+        ix->h_stage_bytes = std::max<size_t>(need, 4096);
+    }
+    uint64_t* off = static_cast<uint64_t*>(ix->h_stage);
+    off[0] = 0;
+    off[1] = n_terms;
+    if (n_terms) std::memcpy(off + 2, terms, size_t(n_terms) * 4);
+    CUDA_TRY(cudaMemcpyAsync(ws->q_off, off, 16, cudaMemcpyHostToDevice, s));
+    if (n_terms) CUDA_TRY(cudaMemcpyAsync(ws->q_terms, off + 2, size_t(n_terms) * 4, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaEventRecord(ev, s));
+    abf_batch b{};
+    b.d_terms = ws->q_terms;
+    b.d_offsets = ws->q_off;
+    b.n_queries = 1;
+    b.path = path;
+    b.d_bitmaps = d_bitmap;
+    b.bitmap_stride_words = round4(n_words_of(ix->n_ads));
+    b.d_ids = d_ids;
+    b.ids_capacity = d_ids ? ids_capacity : 0;
+    b.d_id_offsets = ws->id_off;
+    RunOpts ro;
+    ro.id_counts = d_count;
+    return run_batch(ix, ws, &b, ro, s);
+    API_END
+}
+
+abf_status abf_index_list_bytes(const abf_index* ix, uint64_t* h_out, uint32_t n) {
+    if (!ix || !h_out || n < ix->n_terms) return fail(ABF_ERR_INVALID, "abf_index_list_bytes: bad arguments");
+    std::memcpy(h_out, ix->h_term_bytes.data(), size_t(ix->n_terms) * 8);
+    return ABF_OK;
+}
+
+abf_status abf_profile_enable(abf_index* ix, int on) {
+    API_BEGIN
+    if (!ix) return fail(ABF_ERR_INVALID, "null index");
+    if (on && !ix->prof) ix->prof = new Profiler();
+    ix->prof_on = on != 0;
+    return ABF_OK;
+    API_END
+}
+
+abf_status abf_profile_read(abf_index* ix, abf_kernel_time* out, uint32_t cap, uint32_t* n_out) {
+    API_BEGIN
+    if (!ix || !n_out || (cap && !out)) return fail(ABF_ERR_INVALID, "abf_profile_read: bad arguments");
+    uint64_t launches[K_NKERNELS] = {};
+    double ms[K_NKERNELS] = {};
+    if (ix->prof) {
+        auto* p = static_cast<Profiler*>(ix->prof);
+        for (auto& r : p->recs) {
+            CUDA_TRY(cudaEventSynchronize(r.b));
+            float e = 0;
+            CUDA_TRY(cudaEventElapsedTime(&e, r.a, r.b));
+            ms[r.kid] += e;
+            launches[r.kid] += 1;
+            p->pool.push_back(r.a);
+            p->pool.push_back(r.b);
+        }
+        p->recs.clear();
+    }
+    uint32_t k = 0;
+    for (int i = 0; i < K_NKERNELS; ++i) {
+        if (!launches[i]) continue;
+        if (k < cap) {
+            std::memset(out[k].name, 0, sizeof(out[k].name));
+            std::strncpy(out[k].name, kKernelNames[i], sizeof(out[k].name) - 1);
+            out[k].launches = launches[i];
+            out[k].total_ms = ms[i];
+        }
+        ++k;
+    }
+    *n_out = k;
+    return ABF_OK;
+    API_END
+}
+
+}  // extern "C"

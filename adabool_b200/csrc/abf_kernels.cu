@@ -1,0 +1,808 @@
+// Kernels of libadabool for sm_100a. See abf_kernels.cuh for the overview
+// and abf_internal.h for the list format they decode.
+//
+// Reference counterparts (yxr620/AdaBool):
+//   scatter_kernel / tile_union_kernel  <- ListUnionKernel{1,,Bitset} and
+//       SparseBatchListUnionKernel{1,,Bitset}
+//       (src/AdaBool/load_balance_transformer.cu.h:16-91,138-220) with the
+//       container decoders (src/AdaBool/inverted_list.cu.h:61-130)
+//   probe_kernel  <- KeyBPTransformKernel{1,,Bitset} and
+//       KeyBatchBPTransformKernel_Expanded{1,,Bitset}
+//       (src/AdaBool/key_transformer.cu.h:11-331,
+//        src/AdaBool/key_batch_transformer.cu.h:11-524)
+//   count/scan/write  <- the host loop CollectIdsFromBitmap
+//       (test/adsfilter_batch.cu:82-97)
+#include "abf_kernels.cuh"
+
+#include <algorithm>
+
+namespace abf {
+
+namespace {
+
+constexpr uint32_t kFull = 0xffffffffu;
+constexpr uint32_t kProbeSmemWords = 8192;  // staged term-bitmap words per CTA
+constexpr uint64_t kFlagAgg = 1ull << 62;
+constexpr uint64_t kFlagIncl = 2ull << 62;
+constexpr uint64_t kValMask = (1ull << 62) - 1;
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+__device__ __forceinline__ uint32_t warp_id() { return threadIdx.x >> 5; }
+
+// ---------------------------------------------------------------------------
+// block decode: one warp, one block of up to 128 ids
+// ---------------------------------------------------------------------------
+// Lane j returns the ids of positions 4j..4j+3 of the block (ascending across
+// the warp); position i is valid when i < cnt. The payload is staged in the
+// warp's 512-byte shared buffer with one 16-byte load per lane; each lane
+// extracts its four gaps with a funnel shift, sums them, and a shuffle scan
+// over the lanes turns the gaps into ids.
+__device__ __forceinline__ void decode_block(const IndexView& ix, uint32_t b, uint4* stage, uint32_t (&id)[4],
+                                             uint32_t& cnt) {
+    const uint32_t lane = lane_id();
+    const uint2 d = __ldg(ix.blk_desc + b);
+    const uint32_t first = __ldg(ix.blk_first + b);
+    const uint32_t bits = d.y & 63u;
+    cnt = (d.y >> 8) + 1u;
+    const uint32_t units = ((cnt - 1u) * bits + 127u) >> 7;
+    __syncwarp();
+    if (lane < units) stage[lane] = __ldg(ix.payload + d.x + lane);
+    __syncwarp();
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(stage);
+    const uint32_t mask = bits >= 32u ? kFull : ((1u << bits) - 1u);
+    uint32_t p[4];
+    uint32_t run = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t i = lane * 4u + k;
+        uint32_t g = 0;
+        if (i >= 1u && i < cnt) {
+            uint32_t v = 0;
+            if (bits) {
+                const uint32_t pos = (i - 1u) * bits;
+                const uint32_t wi = pos >> 5;
+                v = __funnelshift_r(w[wi], w[wi + 1], pos & 31u) & mask;
+            }
+            g = v + 1u;
+        }
+        run += g;
+        p[k] = run;
+    }
+    uint32_t incl = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(kFull, incl, o);
+        if (lane >= uint32_t(o)) incl += y;
+    }
+    const uint32_t base = first + (incl - run);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) id[k] = base + p[k];
+}
+
+// OR the decoded ids that fall in [lo, lo + span) into a shared-memory tile.
+// A lane's ids are ascending, so runs in one word are combined before the
+// atomic.
+__device__ __forceinline__ void or_tile(uint32_t* tile, uint32_t lo, uint32_t span, const uint32_t (&id)[4],
+                                        uint32_t cnt) {
+    const uint32_t lane = lane_id();
+    uint32_t cur = kFull, m = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t i = lane * 4u + k;
+        const uint32_t rel = id[k] - lo;
+        if (i < cnt && rel < span) {
+            const uint32_t wd = rel >> 5, bit = 1u << (rel & 31u);
+            if (wd != cur) {
+                if (cur != kFull) atomicOr(tile + cur, m);
+                cur = wd;
+                m = bit;
+            } else {
+                m |= bit;
+            }
+        }
+    }
+    if (cur != kFull) atomicOr(tile + cur, m);
+}
+
+// OR decoded ids (< n_ads) into a global bitmap, same lane-local combining.
+__device__ __forceinline__ void or_global(uint32_t* bm, uint32_t n_ads, const uint32_t (&id)[4], uint32_t cnt) {
+    const uint32_t lane = lane_id();
+    uint32_t cur = kFull, m = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t i = lane * 4u + k;
+        if (i < cnt && id[k] < n_ads) {
+            const uint32_t wd = id[k] >> 5, bit = 1u << (id[k] & 31u);
+            if (wd != cur) {
+                if (cur != kFull) atomicOr(bm + cur, m);
+                cur = wd;
+                m = bit;
+            } else {
+                m |= bit;
+            }
+        }
+    }
+    if (cur != kFull) atomicOr(bm + cur, m);
+}
+
+template <int NT>
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* s_warp, uint32_t* total) {
+    constexpr int NWARP = NT / 32;
+    const uint32_t lane = lane_id(), warp = warp_id();
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(kFull, x, o);
+        if (lane >= uint32_t(o)) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < uint32_t(NWARP) ? s_warp[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(kFull, w, o);
+            if (lane >= uint32_t(o)) w += y;
+        }
+        if (lane < uint32_t(NWARP)) s_warp[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t wex = warp ? s_warp[warp - 1] : 0u;
+    *total = s_warp[NWARP - 1];
+    __syncthreads();
+    return wex + x - v;
+}
+
+template <int NT>
+__device__ __forceinline__ uint64_t block_sum_u64(uint64_t v, unsigned long long* s) {
+    const uint32_t lane = lane_id(), warp = warp_id();
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFull, v, o);
+    if (lane == 0) s[warp] = v;
+    __syncthreads();
+    uint64_t t = 0;
+    for (int i = 0; i < NT / 32; ++i) t += s[i];
+    __syncthreads();
+    return t;
+}
+
+// first index in [a, b) with arr[index] >= key (arr ascending)
+__device__ __forceinline__ uint32_t lower_bound_g(const uint32_t* arr, uint32_t a, uint32_t b, uint32_t key) {
+    while (a < b) {
+        const uint32_t m = (a + b) >> 1;
+        if (__ldg(arr + m) < key) a = m + 1; else b = m;
+    }
+    return a;
+}
+
+// ---------------------------------------------------------------------------
+// mbarrier + bulk async copy (TMA engine, 1-D form)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// ---------------------------------------------------------------------------
+// planning
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) plan_kernel(IndexView ix, PlanArgs a) {
+    __shared__ uint32_t s_warp[32];
+    __shared__ unsigned long long s_red[8];
+    __shared__ uint32_t s_path;
+    const uint32_t tid = threadIdx.x;
+    for (uint32_t q = blockIdx.x; q < a.n_q; q += gridDim.x) {
+        uint64_t qb = a.q_off[q], qe = a.q_off[q + 1];
+        if (qe < qb || qe > a.max_terms) {
+            // offsets outside the scratch arrays: the query gets no work
+            if (tid == 0 && a.err) atomicOr(a.err, kErrTermRange);
+            qe = qb = 0;
+        }
+        uint32_t path = a.paths ? a.paths[q] : a.path_uniform;
+        if (path == ABF_PATH_AUTO) {
+            // fixed rule: probe when the query's lists cover more than
+            // probe_min_frac of all blocks
+            uint64_t nb = 0;
+            for (uint64_t i = qb + tid; i < qe; i += 256) {
+                const uint32_t t = a.terms[i];
+                if (t < ix.n_terms) nb += __ldg(ix.term_blk + t + 1) - __ldg(ix.term_blk + t);
+            }
+            nb = block_sum_u64<256>(nb, s_red);
+            path = (double(nb) > double(a.probe_min_frac) * double(ix.n_blocks)) ? ABF_PATH_PROBE : ABF_PATH_UNION;
+        }
+        if (tid == 0) {
+            if (path == ABF_PATH_PROBE) {
+                const uint32_t slot = atomicAdd(a.n_probe, 1u);
+                if (slot < a.probe_cap) a.probe_list[slot] = q;
+                else path = ABF_PATH_UNION;  // no probe slot left: same result by list-union
+            }
+            s_path = path;
+        }
+        __syncthreads();
+        path = s_path;
+        const uint32_t hm = path == ABF_PATH_TILE ? 0u : (path == ABF_PATH_HYBRID ? a.hybrid_min : kNoHeavy);
+        const bool probe = path == ABF_PATH_PROBE;
+        uint32_t carry = 0;
+        for (uint64_t c0 = qb; c0 < qe; c0 += 256) {
+            const uint64_t i = c0 + tid;
+            uint32_t cnt = 0;
+            if (i < qe && !probe) {
+                const uint32_t t = a.terms[i];
+                if (t < ix.n_terms && __ldg(ix.term_len + t) < hm)
+                    cnt = __ldg(ix.term_blk + t + 1) - __ldg(ix.term_blk + t);
+            }
+            uint32_t tot;
+            const uint32_t ex = block_excl_scan<256>(cnt, s_warp, &tot);
+            if (i < qe) a.term_lpref[i] = carry + ex;
+            carry += tot;
+        }
+        if (tid == 0) {
+            a.heavy_min[q] = probe ? kNoHeavy : hm;
+            a.q_light_cnt[q] = carry;
+            if (a.path_out) a.path_out[q] = uint8_t(path);
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(1024) queue_scan_kernel(QueueArgs a) {
+    __shared__ unsigned long long s_warp[32];
+    __shared__ unsigned long long s_carry;
+    const uint32_t tid = threadIdx.x, lane = lane_id(), warp = warp_id();
+    if (tid == 0) s_carry = 0;
+    __syncthreads();
+    for (uint32_t c0 = 0; c0 < a.n_q; c0 += 1024) {
+        const uint32_t i = c0 + tid;
+        const uint64_t v = i < a.n_q ? a.q_light_cnt[i] : 0ull;
+        uint64_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t y = __shfl_up_sync(kFull, x, o);
+            if (lane >= uint32_t(o)) x += y;
+        }
+        if (lane == 31) s_warp[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            uint64_t w = s_warp[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint64_t y = __shfl_up_sync(kFull, w, o);
+                if (lane >= uint32_t(o)) w += y;
+            }
+            s_warp[lane] = w;
+        }
+        __syncthreads();
+        const uint64_t base = s_carry + (warp ? s_warp[warp - 1] : 0ull);
+        if (i < a.n_q) a.q_light_pref[i] = base + x - v;
+        __syncthreads();
+        if (tid == 0) s_carry += s_warp[31];
+        __syncthreads();
+    }
+    if (tid == 0) a.q_light_pref[a.n_q] = s_carry;
+}
+
+__global__ void __launch_bounds__(256) probe_bits_kernel(ProbeBitsArgs a) {
+    const uint32_t slot = blockIdx.x;
+    if (slot >= *a.n_probe) return;
+    const uint32_t q = a.probe_list[slot];
+    uint32_t* bm = a.qbm + slot * a.qbm_stride;
+    for (uint64_t i = a.q_off[q] + threadIdx.x; i < a.q_off[q + 1]; i += blockDim.x) {
+        const uint32_t t = a.terms[i];
+        if (t < a.n_terms) atomicOr(bm + (t >> 5), 1u << (t & 31u));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// list-union, merge variant
+// ---------------------------------------------------------------------------
+template <int W, int NW>
+__global__ void __launch_bounds__(NW * 32) tile_union_kernel(IndexView ix, TileArgs a) {
+    constexpr int NT = NW * 32;
+    constexpr uint32_t SPAN = uint32_t(W) * 32u;
+    __shared__ uint32_t tile[W];
+    __shared__ __align__(16) uint4 stage[NW][32];
+    __shared__ uint32_t s_lo[NT];
+    __shared__ uint32_t s_pref[NT + 1];
+    __shared__ uint32_t s_warp[32];
+    const uint32_t tid = threadIdx.x, warp = warp_id();
+    const uint64_t items = uint64_t(a.n_q) * a.n_tiles;
+    for (uint64_t item = blockIdx.x; item < items; item += gridDim.x) {
+        const uint32_t q = uint32_t(item / a.n_tiles);
+        const uint32_t t = uint32_t(item - uint64_t(q) * a.n_tiles);
+        const uint32_t lo_id = t * SPAN;
+        const uint32_t hi_id = (uint64_t(lo_id) + SPAN > ix.n_ads) ? ix.n_ads : lo_id + SPAN;
+        const uint32_t hm = a.heavy_min ? a.heavy_min[q] : a.heavy_all;
+        const uint64_t qb = a.q_off[q], qe = a.q_off[q + 1];
+        if (a.accumulate && (hm == kNoHeavy || qb == qe)) continue;  // nothing to OR in
+        uint32_t* dst = a.out + uint64_t(q) * a.out_stride + uint64_t(t) * W;
+        const uint64_t left = a.n_words - uint64_t(t) * W;
+        const uint32_t nw = left < uint64_t(W) ? uint32_t(left) : uint32_t(W);
+        for (uint32_t i = tid; i < uint32_t(W); i += NT) tile[i] = (a.accumulate && i < nw) ? dst[i] : 0u;
+        __syncthreads();
+        if (hm != kNoHeavy) {
+            for (uint64_t c0 = qb; c0 < qe; c0 += NT) {
+                const uint64_t i = c0 + tid;
+                uint32_t lo = 0, cnt = 0;
+                if (i < qe) {
+                    const uint32_t term = a.terms[i];
+                    if (term < ix.n_terms && __ldg(ix.term_len + term) >= hm) {
+                        const uint32_t b0 = __ldg(ix.term_blk + term), b1 = __ldg(ix.term_blk + term + 1);
+                        lo = lower_bound_g(ix.blk_last, b0, b1, lo_id);
+                        const uint32_t hi = lower_bound_g(ix.blk_first, lo, b1, hi_id);
+                        cnt = hi - lo;
+                    }
+                }
+                uint32_t total;
+                const uint32_t ex = block_excl_scan<NT>(cnt, s_warp, &total);
+                s_lo[tid] = lo;
+                s_pref[tid] = ex;
+                if (tid == NT - 1) s_pref[NT] = ex + cnt;
+                __syncthreads();
+                for (uint32_t f = warp; f < total; f += NW) {
+                    // slot s: s_pref[s] <= f < s_pref[s+1]
+                    uint32_t a0 = 0, a1 = NT;
+                    while (a1 - a0 > 1) {
+                        const uint32_t m = (a0 + a1) >> 1;
+                        if (s_pref[m] <= f) a0 = m; else a1 = m;
+                    }
+                    const uint32_t b = s_lo[a0] + (f - s_pref[a0]);
+                    uint32_t id[4], cnt_b;
+                    decode_block(ix, b, stage[warp], id, cnt_b);
+                    or_tile(tile, lo_id, SPAN, id, cnt_b);
+                }
+                __syncthreads();
+            }
+        }
+        for (uint32_t i = tid; i < nw; i += NT) dst[i] = tile[i];
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// list-union, scatter variant (load-balanced over the short lists' blocks)
+// ---------------------------------------------------------------------------
+template <int NW>
+__global__ void __launch_bounds__(NW * 32) scatter_kernel(IndexView ix, ScatterArgs a) {
+    __shared__ __align__(16) uint4 stage[NW][32];
+    const uint32_t warp = warp_id();
+    const uint64_t total = a.q_light_pref[a.n_q];
+    const uint64_t bpw = a.blocks_per_warp;
+    const uint64_t nwt = uint64_t(gridDim.x) * NW;
+    for (uint64_t f0 = (uint64_t(blockIdx.x) * NW + warp) * bpw; f0 < total; f0 += nwt * bpw) {
+        const uint64_t f1 = f0 + bpw < total ? f0 + bpw : total;
+        // query: last q with q_light_pref[q] <= f0
+        uint32_t q0 = 0, q1 = a.n_q;
+        while (q1 - q0 > 1) {
+            const uint32_t m = (q0 + q1) >> 1;
+            if (a.q_light_pref[m] <= f0) q0 = m; else q1 = m;
+        }
+        uint32_t q = q0;
+        uint64_t qb = a.q_off[q], qe = a.q_off[q + 1];
+        uint32_t qtot = uint32_t(a.q_light_pref[q + 1] - a.q_light_pref[q]);
+        const uint32_t r = uint32_t(f0 - a.q_light_pref[q]);
+        // term slot: last i with term_lpref[i] <= r
+        uint64_t i0 = qb, i1 = qe;
+        while (i1 - i0 > 1) {
+            const uint64_t m = (i0 + i1) >> 1;
+            if (a.term_lpref[m] <= r) i0 = m; else i1 = m;
+        }
+        uint64_t i = i0;
+        uint32_t j = r - a.term_lpref[i];
+        uint32_t* out = a.out + uint64_t(a.out_slot ? a.out_slot[q] : q) * a.out_stride;
+        for (uint64_t f = f0; f < f1;) {
+            const uint32_t nb = (i + 1 < qe ? a.term_lpref[i + 1] : qtot) - a.term_lpref[i];
+            if (j < nb) {
+                const uint32_t b = __ldg(ix.term_blk + a.terms[i]) + j;
+                uint32_t id[4], cnt;
+                decode_block(ix, b, stage[warp], id, cnt);
+                or_global(out, ix.n_ads, id, cnt);
+                ++j;
+                ++f;
+            } else {
+                ++i;
+                j = 0;
+                if (i >= qe) {
+                    do {
+                        ++q;
+                    } while (a.q_light_pref[q + 1] == a.q_light_pref[q]);
+                    qb = a.q_off[q];
+                    qe = a.q_off[q + 1];
+                    qtot = uint32_t(a.q_light_pref[q + 1] - a.q_light_pref[q]);
+                    i = qb;
+                    out = a.out + uint64_t(a.out_slot ? a.out_slot[q] : q) * a.out_stride;
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// bitmap-probe
+// ---------------------------------------------------------------------------
+template <int NW>
+__global__ void __launch_bounds__(NW * 32) probe_kernel(IndexView ix, ProbeArgs a) {
+    __shared__ __align__(128) uint32_t sbm[kProbeSmemWords];
+    __shared__ __align__(16) uint4 stage[NW][32];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t s_fail;
+    const uint32_t tid = threadIdx.x, lane = lane_id(), warp = warp_id();
+    const uint32_t n_probe = a.d_n_probe ? *a.d_n_probe : a.n_probe_host;
+    if (n_probe == 0 || ix.n_blocks == 0) return;
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+        s_fail = 0;
+    }
+    __syncthreads();
+    uint32_t phase = 0;
+    const uint64_t cb = a.chunk_blocks;
+    const uint64_t n_chunks = (ix.n_blocks + cb - 1) / cb;
+    for (uint64_t chunk = blockIdx.x; chunk < n_chunks; chunk += gridDim.x) {
+        const uint64_t c0 = chunk * cb;
+        const uint64_t c1 = c0 + cb < ix.n_blocks ? c0 + cb : ix.n_blocks;
+        const uint32_t t0 = __ldg(ix.blk_term + c0), t1 = __ldg(ix.blk_term + c1 - 1);
+        const uint32_t w0 = (t0 >> 5) & ~3u;
+        uint32_t w1 = ((t1 >> 5) + 4u) & ~3u;
+        if (w1 > a.qbm_words) w1 = a.qbm_words;
+        const uint32_t span = w1 > w0 ? w1 - w0 : 0u;
+        for (uint32_t g0 = 0; g0 < n_probe; g0 += kProbeGroup) {
+            const uint32_t G = n_probe - g0 < kProbeGroup ? n_probe - g0 : kProbeGroup;
+            const bool staged = a.staged_ok && span > 0 && (span & 3u) == 0 && span * G <= kProbeSmemWords;
+            if (staged) {
+                __syncthreads();  // everyone is done with the previous slice
+                if (tid == 0) {
+                    fence_proxy_async();
+                    mbar_expect_tx(&bar, span * 4u * G);
+                    for (uint32_t g = 0; g < G; ++g)
+                        bulk_g2s(sbm + g * span, a.qbm + uint64_t(g0 + g) * a.qbm_stride + w0, span * 4u, &bar);
+                }
+                uint32_t spins = 0;
+                while (!mbar_try_wait(&bar, phase)) {
+                    if (++spins > kSpinLimit) {
+                        s_fail = 1;
+                        break;
+                    }
+                }
+                phase ^= 1u;
+                if (__syncthreads_or(s_fail)) {
+                    if (tid == 0) atomicOr(a.err, kErrTmaTimeout);
+                    return;
+                }
+            }
+            for (uint64_t base = c0 + uint64_t(warp) * 128u; base < c1; base += uint64_t(NW) * 128u) {
+                const uint64_t idx = base + lane * 4u;
+                uint32_t tv[4];
+                if (idx + 3 < c1) {
+                    const uint4 v = __ldg(reinterpret_cast<const uint4*>(ix.blk_term + idx));
+                    tv[0] = v.x; tv[1] = v.y; tv[2] = v.z; tv[3] = v.w;
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) tv[k] = idx + k < c1 ? __ldg(ix.blk_term + idx + k) : kFull;
+                }
+                uint32_t hit[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    uint32_t m = 0;
+                    const uint32_t term = tv[k];
+                    if (term != kFull) {
+                        const uint32_t wd = term >> 5, bit = term & 31u;
+                        if (wd < a.qbm_words) {
+                            for (uint32_t g = 0; g < G; ++g) {
+                                const uint32_t word = staged ? sbm[g * span + (wd - w0)]
+                                                             : __ldg(a.qbm + uint64_t(g0 + g) * a.qbm_stride + wd);
+                                m |= ((word >> bit) & 1u) << g;
+                            }
+                        }
+                    }
+                    hit[k] = m;
+                }
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    uint32_t lanes = __ballot_sync(kFull, hit[k] != 0u);
+                    while (lanes) {
+                        const uint32_t src = __ffs(lanes) - 1u;
+                        lanes &= lanes - 1u;
+                        uint32_t qm = __shfl_sync(kFull, hit[k], src);
+                        const uint32_t b = uint32_t(base + src * 4u + k);
+                        uint32_t id[4], cnt;
+                        decode_block(ix, b, stage[warp], id, cnt);
+                        while (qm) {
+                            const uint32_t g = __ffs(qm) - 1u;
+                            qm &= qm - 1u;
+                            const uint32_t slot = g0 + g;
+                            const uint32_t o = a.out_slot ? a.out_slot[slot] : slot;
+                            or_global(a.out + uint64_t(o) * a.out_stride, ix.n_ads, id, cnt);
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// compaction: count, decoupled look-back scan, write
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t masked_word(const uint32_t* bm, uint64_t w, uint64_t n_bits) {
+    uint32_t v = bm[w];
+    const uint64_t lo = w * 32u;
+    if (lo + 32u > n_bits) v &= (n_bits > lo) ? ((1u << uint32_t(n_bits - lo)) - 1u) : 0u;
+    return v;
+}
+
+__global__ void __launch_bounds__(256) count_kernel(CompactArgs a) {
+    __shared__ unsigned long long s_red[8];
+    const uint64_t n_words = (a.n_bits + 31) / 32;
+    const uint64_t items = uint64_t(a.n_q) * a.n_chunks;
+    for (uint64_t item = blockIdx.x; item < items; item += gridDim.x) {
+        const uint32_t q = uint32_t(item / a.n_chunks);
+        const uint32_t c = uint32_t(item - uint64_t(q) * a.n_chunks);
+        const uint32_t* bm = a.bm + uint64_t(q) * a.stride;
+        const uint64_t w0 = uint64_t(c) * kCompactChunkWords;
+        const uint64_t w1 = w0 + kCompactChunkWords < n_words ? w0 + kCompactChunkWords : n_words;
+        uint64_t s = 0;
+        for (uint64_t w = w0 + threadIdx.x; w < w1; w += 256) s += __popc(masked_word(bm, w, a.n_bits));
+        s = block_sum_u64<256>(s, s_red);
+        if (threadIdx.x == 0) a.counts[item] = uint32_t(s);
+    }
+}
+
+constexpr int kScanNT = 256;
+constexpr int kScanIPT = int(kScanTile) / kScanNT;
+
+__global__ void __launch_bounds__(kScanNT) scan_kernel(const uint32_t* in, uint64_t n, uint64_t* out, uint64_t* status,
+                                                      uint32_t* counter, uint32_t* err) {
+    __shared__ uint32_t s_tile;
+    __shared__ unsigned long long s_prefix;
+    __shared__ uint32_t s_warp[32];
+    const uint32_t tid = threadIdx.x;
+    if (tid == 0) s_tile = atomicAdd(counter, 1u);
+    __syncthreads();
+    const uint64_t tile = s_tile;
+    const uint64_t base = tile * kScanTile + uint64_t(tid) * kScanIPT;
+    uint32_t v[kScanIPT];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanIPT; ++k) {
+        v[k] = base + k < n ? in[base + k] : 0u;
+        sum += v[k];
+    }
+    uint32_t agg;
+    const uint32_t ex = block_excl_scan<kScanNT>(sum, s_warp, &agg);
+    if (tid == 0) {
+        uint64_t prefix = 0;
+        if (tile == 0) {
+            __threadfence();
+            atomicExch(reinterpret_cast<unsigned long long*>(status), (unsigned long long)(kFlagIncl | agg));
+        } else {
+            __threadfence();
+            atomicExch(reinterpret_cast<unsigned long long*>(status + tile), (unsigned long long)(kFlagAgg | agg));
+            uint64_t k = tile - 1;
+            uint32_t spins = 0;
+            for (;;) {
+                const uint64_t s = *reinterpret_cast<volatile unsigned long long*>(status + k);
+                const uint64_t f = s & ~kValMask;
+                if (f == 0) {
+                    if (++spins > kSpinLimit) {
+                        atomicOr(err, kErrScanTimeout);
+                        break;
+                    }
+                    __nanosleep(32);
+                    continue;
+                }
+                prefix += s & kValMask;
+                if (f == kFlagIncl || k == 0) break;
+                --k;
+            }
+            __threadfence();
+            atomicExch(reinterpret_cast<unsigned long long*>(status + tile),
+                       (unsigned long long)(kFlagIncl | (prefix + agg)));
+        }
+        s_prefix = prefix;
+    }
+    __syncthreads();
+    uint64_t run = s_prefix + ex;
+#pragma unroll
+    for (int k = 0; k < kScanIPT; ++k) {
+        if (base + k < n) out[base + k] = run;
+        run += v[k];
+    }
+    const uint64_t last_tile = (n - 1) / kScanTile;
+    if (tile == last_tile && tid == 0) out[n] = s_prefix + agg;
+}
+
+__global__ void __launch_bounds__(256) write_ids_kernel(CompactArgs a) {
+    __shared__ uint32_t s_ids[256 * 32];
+    __shared__ uint32_t s_warp[32];
+    const uint32_t tid = threadIdx.x;
+    const uint64_t n_words = (a.n_bits + 31) / 32;
+    const uint64_t items = uint64_t(a.n_q) * a.n_chunks;
+    for (uint64_t item = blockIdx.x; item < items; item += gridDim.x) {
+        const uint32_t q = uint32_t(item / a.n_chunks);
+        const uint32_t c = uint32_t(item - uint64_t(q) * a.n_chunks);
+        const uint32_t* bm = a.bm + uint64_t(q) * a.stride;
+        uint64_t out = a.offsets[item];
+        if (c == 0 && tid == 0) {
+            if (a.id_offsets) a.id_offsets[q] = out;
+            if (a.id_counts) a.id_counts[q] = a.offsets[item + a.n_chunks] - out;
+            if (a.id_offsets && q == a.n_q - 1) a.id_offsets[a.n_q] = a.offsets[items];
+        }
+        const uint64_t w0 = uint64_t(c) * kCompactChunkWords;
+        const uint64_t w1 = w0 + kCompactChunkWords < n_words ? w0 + kCompactChunkWords : n_words;
+        for (uint64_t r0 = w0; r0 < w1; r0 += 256) {
+            const uint64_t w = r0 + tid;
+            uint32_t v = w < w1 ? masked_word(bm, w, a.n_bits) : 0u;
+            uint32_t tot;
+            uint32_t pos = block_excl_scan<256>(__popc(v), s_warp, &tot);
+            const uint32_t idbase = uint32_t(w * 32u);
+            while (v) {
+                const uint32_t b = __ffs(v) - 1u;
+                v &= v - 1u;
+                s_ids[pos++] = idbase + b;
+            }
+            __syncthreads();
+            for (uint32_t k = tid; k < tot; k += 256) {
+                const uint64_t o = out + k;
+                if (o < a.capacity) a.ids[o] = s_ids[k];
+            }
+            out += tot;
+            __syncthreads();
+        }
+    }
+}
+
+inline int grid_for(uint64_t items, int sm_count, uint32_t per_sm) {
+    uint64_t g = uint64_t(sm_count) * (per_sm ? per_sm : 1u);
+    if (items < g) g = items;
+    return int(g ? g : 1);
+}
+
+}  // namespace
+
+IndexView view_of(const abf_index* ix) {
+    IndexView v;
+    v.payload = reinterpret_cast<const uint4*>(ix->dev.payload);
+    v.blk_first = ix->dev.blk_first;
+    v.blk_last = ix->dev.blk_last;
+    v.blk_desc = reinterpret_cast<const uint2*>(ix->dev.blk_desc);
+    v.blk_term = ix->dev.blk_term;
+    v.term_blk = ix->dev.term_blk;
+    v.term_len = ix->dev.term_len;
+    v.n_terms = ix->n_terms;
+    v.n_ads = ix->n_ads;
+    v.n_blocks = ix->n_blocks;
+    return v;
+}
+
+uint32_t compact_chunks(uint64_t n_bits) {
+    const uint64_t n_words = (n_bits + 31) / 32;
+    return uint32_t((n_words + kCompactChunkWords - 1) / kCompactChunkWords);
+}
+uint64_t scan_tiles(uint64_t n) { return (n + kScanTile - 1) / kScanTile; }
+
+cudaError_t launch_plan(const IndexView& v, const PlanArgs& a, cudaStream_t s) {
+    if (a.n_q == 0) return cudaSuccess;
+    const uint32_t g = a.n_q < 65535u * 16u ? a.n_q : 65535u * 16u;
+    plan_kernel<<<g, 256, 0, s>>>(v, a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_queue_scan(const QueueArgs& a, cudaStream_t s) {
+    queue_scan_kernel<<<1, 1024, 0, s>>>(a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_probe_bits(const ProbeBitsArgs& a, uint32_t probe_cap, cudaStream_t s) {
+    if (probe_cap == 0) return cudaSuccess;
+    probe_bits_kernel<<<probe_cap, 256, 0, s>>>(a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <int W>
+static cudaError_t tile_dispatch_w(const IndexView& v, const TileArgs& a, uint32_t nw, int grid, cudaStream_t s) {
+    switch (nw) {
+        case 1: tile_union_kernel<W, 1><<<grid, 32, 0, s>>>(v, a); break;
+        case 2: tile_union_kernel<W, 2><<<grid, 64, 0, s>>>(v, a); break;
+        case 4: tile_union_kernel<W, 4><<<grid, 128, 0, s>>>(v, a); break;
+        default: tile_union_kernel<W, 8><<<grid, 256, 0, s>>>(v, a); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tile_union(const IndexView& v, const TileArgs& a, const abf_tuning& t, int sm_count,
+                              cudaStream_t s) {
+    const uint64_t items = uint64_t(a.n_q) * a.n_tiles;
+    if (items == 0) return cudaSuccess;
+    const uint32_t nw = t.warps_per_tile ? t.warps_per_tile : 8u;
+    // ctas_per_sm counts 8-warp CTAs; narrower CTAs are packed proportionally
+    const uint32_t per_sm = (t.ctas_per_sm ? t.ctas_per_sm : 2u) * (nw >= 8u ? 1u : 8u / nw);
+    const int grid = grid_for(items, sm_count, per_sm);
+    cudaError_t e;
+    switch (t.tile_words) {
+        case 256: e = tile_dispatch_w<256>(v, a, nw, grid, s); break;
+        case 512: e = tile_dispatch_w<512>(v, a, nw, grid, s); break;
+        default: e = tile_dispatch_w<1024>(v, a, nw, grid, s); break;
+    }
+    count_launch();
+    return e;
+}
+
+cudaError_t launch_scatter(const IndexView& v, const ScatterArgs& a, const abf_tuning& t, int sm_count,
+                           cudaStream_t s) {
+    if (a.n_q == 0) return cudaSuccess;
+    const int grid = grid_for(~0ull, sm_count, t.ctas_per_sm ? t.ctas_per_sm * 2u : 8u);
+    scatter_kernel<8><<<grid, 256, 0, s>>>(v, a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_probe(const IndexView& v, const ProbeArgs& a, const abf_tuning& t, int sm_count, cudaStream_t s) {
+    if (v.n_blocks == 0) return cudaSuccess;
+    const uint64_t n_chunks = (v.n_blocks + a.chunk_blocks - 1) / a.chunk_blocks;
+    const int grid = grid_for(n_chunks, sm_count, t.ctas_per_sm ? t.ctas_per_sm : 4u);
+    probe_kernel<8><<<grid, 256, 0, s>>>(v, a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_compact_count(const CompactArgs& a, int sm_count, cudaStream_t s) {
+    const uint64_t items = uint64_t(a.n_q) * a.n_chunks;
+    if (items == 0) return cudaSuccess;
+    count_kernel<<<grid_for(items, sm_count, 8), 256, 0, s>>>(a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_compact_scan(const CompactArgs& a, cudaStream_t s) {
+    const uint64_t items = uint64_t(a.n_q) * a.n_chunks;
+    if (items == 0) return cudaSuccess;
+    const uint64_t tiles = scan_tiles(items);
+    cudaError_t e = cudaMemsetAsync(a.scan_status, 0, tiles * sizeof(uint64_t), s);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(a.scan_counter, 0, sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
+    scan_kernel<<<unsigned(tiles), kScanNT, 0, s>>>(a.counts, items, a.offsets, a.scan_status, a.scan_counter,
+                                                    a.err);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_compact_write(const CompactArgs& a, int sm_count, cudaStream_t s) {
+    const uint64_t items = uint64_t(a.n_q) * a.n_chunks;
+    if (items == 0) return cudaSuccess;
+    write_ids_kernel<<<grid_for(items, sm_count, 4), 256, 0, s>>>(a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace abf

@@ -1,0 +1,147 @@
+// Kernel argument blocks and launchers of libadabool (sm_100a).
+//
+// Kernels (all integer, HBM/L2 bound):
+//   plan_kernel        per query: resolve the path, split lists into merged
+//                      (long) and scattered (short), prefix the short lists'
+//                      block counts, claim bitmap-probe slots
+//   queue_scan_kernel  exclusive scan of the per-query scattered block counts
+//   probe_bits_kernel  term bitmaps of the queries routed to the probe
+//   tile_union_kernel  list-union, merge variant: one CTA owns a tile of one
+//                      query's output bitmap in shared memory, decodes every
+//                      block of the long lists that overlaps the tile, ORs
+//                      with shared-memory atomics and writes the tile once
+//   scatter_kernel     list-union, scatter variant: load-balanced warps decode
+//                      the short lists' blocks and OR into the global bitmap
+//                      with lane-combined atomicOr
+//   probe_kernel       bitmap-probe: scans every block of the index, stages
+//                      the probe queries' term-bitmap slices in shared memory
+//                      with bulk async copies (TMA engine), tests each block's
+//                      term and scatters hit blocks into their queries
+//   count/scan/write   compaction: bitmap -> ascending uint32 ids
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "abf_internal.h"
+
+namespace abf {
+
+constexpr uint32_t kNoHeavy = 0xffffffffu;   // heavy_min meaning "merge no list"
+constexpr uint32_t kCompactChunkWords = 2048; // bitmap words per compaction work item
+constexpr uint32_t kProbeGroup = 32;          // probe queries tested per pass
+constexpr uint32_t kScanTile = 2048;          // elements per decoupled look-back tile
+
+// device error codes (workspace flag)
+constexpr uint32_t kErrScanTimeout = 1u;
+constexpr uint32_t kErrTmaTimeout = 2u;
+constexpr uint32_t kErrTermRange = 4u;
+
+struct PlanArgs {
+    const uint32_t* terms;
+    const uint64_t* q_off;
+    uint32_t n_q;
+    const uint8_t* paths;     // per-query abf_path or null
+    uint32_t path_uniform;    // abf_path when paths is null
+    uint32_t hybrid_min;      // HYBRID merge threshold (postings)
+    float probe_min_frac;     // fixed rule: probe when touched blocks / all blocks > this
+    uint32_t* heavy_min;      // out: per query
+    uint32_t* term_lpref;     // out: per term slot, exclusive prefix of scattered blocks
+    uint64_t* q_light_cnt;    // out: per query scattered blocks
+    uint32_t* probe_list;     // out: probe slot -> query
+    uint32_t* n_probe;        // in/out: zeroed before launch
+    uint32_t probe_cap;
+    uint8_t* path_out;        // out (optional): resolved path per query
+    uint64_t max_terms;       // term slots of the scratch arrays; queries past it get no work
+    uint32_t* err;            // device error flag (optional)
+};
+
+struct QueueArgs {
+    const uint64_t* q_light_cnt;
+    uint64_t* q_light_pref;   // n_q + 1
+    uint32_t n_q;
+};
+
+struct ProbeBitsArgs {
+    const uint32_t* terms;
+    const uint64_t* q_off;
+    const uint32_t* probe_list;
+    const uint32_t* n_probe;
+    uint32_t* qbm;            // probe_cap x qbm_stride words, zeroed before launch
+    uint64_t qbm_stride;
+    uint32_t n_terms;
+};
+
+struct TileArgs {
+    const uint32_t* terms;
+    const uint64_t* q_off;
+    const uint32_t* heavy_min; // per query (null: heavy_all for every query)
+    uint32_t heavy_all;
+    uint32_t n_q;
+    uint32_t n_tiles;
+    uint32_t* out;
+    uint64_t out_stride;      // words between query bitmaps
+    uint64_t n_words;         // words of one bitmap
+    int accumulate;           // 1: OR into the existing bitmap, 0: overwrite
+};
+
+struct ScatterArgs {
+    const uint32_t* terms;
+    const uint64_t* q_off;
+    const uint32_t* term_lpref;
+    const uint64_t* q_light_pref; // n_q + 1
+    uint32_t n_q;
+    const uint32_t* out_slot;  // query -> output bitmap index (null: identity)
+    uint32_t* out;
+    uint64_t out_stride;
+    uint32_t blocks_per_warp;
+};
+
+struct ProbeArgs {
+    const uint32_t* qbm;       // probe term bitmaps, qbm_stride words apart
+    uint64_t qbm_stride;
+    uint32_t qbm_words;        // readable words per bitmap
+    int staged_ok;             // qbm 16-byte aligned and stride % 4 == 0
+    const uint32_t* d_n_probe; // device count (null: n_probe_host)
+    uint32_t n_probe_host;
+    const uint32_t* out_slot;  // probe slot -> output bitmap index (null: identity)
+    uint32_t* out;
+    uint64_t out_stride;
+    uint32_t chunk_blocks;     // multiple of 128
+    uint32_t* err;
+};
+
+struct CompactArgs {
+    const uint32_t* bm;
+    uint64_t stride;           // words between bitmaps
+    uint32_t n_q;
+    uint64_t n_bits;           // ids >= n_bits are dropped
+    uint32_t n_chunks;         // per bitmap
+    uint32_t* counts;          // n_q * n_chunks
+    uint64_t* offsets;         // n_q * n_chunks + 1
+    uint64_t* scan_status;     // per scan tile
+    uint32_t* scan_counter;
+    uint32_t* ids;
+    uint64_t capacity;
+    uint64_t* id_offsets;      // optional n_q + 1
+    uint64_t* id_counts;       // optional n_q
+    uint32_t* err;
+};
+
+IndexView view_of(const abf_index* ix);
+uint32_t compact_chunks(uint64_t n_bits);
+uint64_t scan_tiles(uint64_t n);
+
+cudaError_t launch_plan(const IndexView& v, const PlanArgs& a, cudaStream_t s);
+cudaError_t launch_queue_scan(const QueueArgs& a, cudaStream_t s);
+cudaError_t launch_probe_bits(const ProbeBitsArgs& a, uint32_t probe_cap, cudaStream_t s);
+cudaError_t launch_tile_union(const IndexView& v, const TileArgs& a, const abf_tuning& t, int sm_count,
+                              cudaStream_t s);
+cudaError_t launch_scatter(const IndexView& v, const ScatterArgs& a, const abf_tuning& t, int sm_count,
+                           cudaStream_t s);
+cudaError_t launch_probe(const IndexView& v, const ProbeArgs& a, const abf_tuning& t, int sm_count,
+                         cudaStream_t s);
+cudaError_t launch_compact_count(const CompactArgs& a, int sm_count, cudaStream_t s);
+cudaError_t launch_compact_scan(const CompactArgs& a, cudaStream_t s);
+cudaError_t launch_compact_write(const CompactArgs& a, int sm_count, cudaStream_t s);
+
+}  // namespace abf

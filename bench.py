@@ -1,0 +1,492 @@
+#!/usr/bin/env python
+"""Benchmark of the Boolean-filtering hot path on one or more B200s.
+
+Workload (default, config c1): a synthetic filter matrix of 2^20 terms x 2^24
+ads with ~500M postings (Zipf(1.05) list lengths clipped to [1, 5M], uniform
+sorted unique ad ids per list) and 2,048 queries of distinct terms (lognormal
+term counts, median 40, sigma 1.5, clipped to [1, 5000]; terms drawn with
+probability proportional to list length). One step answers every query:
+bitmap (2^24 bits) plus sorted uint32 id list per query, through the batched
+API in sub-batches. Inputs are larger than L2 (the compressed index alone is
+~0.8 GB), so no flush is needed between steps.
+
+  value  queries/s with inputs already in HBM (device-timed, CUDA events)
+  e2e    the same through the public API from pinned host buffers: per
+         sub-batch the query terms go host->device and every id list comes
+         back device->host inside the timed region
+
+Multi-GPU: replicas (each rank its own query set on its own copy of the
+index, no collective on the data path), launched by torchrun; the time is
+the max over ranks.
+
+`--impl reference` times the reference's own CPU path (ComputeGroundTruth,
+test/adsfilter_q_all.cu:196-208, built from the reference sources into
+oracle/_ref) on the host cores, on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "batched queries/s & postings GB/s vs HBM peak; learned vs fixed path planner"
+UNIT = "queries/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--config", default="c1")
+    p.add_argument("--scale", type=float, default=1.0, help="shrink the workload (profiling / quick runs)")
+    p.add_argument("--queries", type=int, default=0, help="override the query count")
+    p.add_argument("--sub-batch", type=int, default=64)
+    p.add_argument("--path", default="hybrid", choices=["auto", "probe", "union", "hybrid", "tile", "planner"])
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--out", default="", help="also append the JSON line to this file")
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+def peaks():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of the SM clock and throttle reasons while running."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = max(mx, float(f[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def make_workload(cfg_name: str, scale: float, n_queries: int, rank: int):
+    from adabool_b200 import workload as W
+    cfg = W.CONFIGS[cfg_name]
+    if scale != 1.0:
+        cfg = W.scaled(cfg, scale)
+    q = cfg.queries
+    if n_queries:
+        q.n_queries = n_queries
+    q.seed = q.seed + 1000 * rank
+    t0 = time.time()
+    off, ads = W.gen_lists(cfg.lists)
+    lens = np.diff(off).astype(np.uint32)
+    qoff, qterms = W.gen_queries(q, lens)
+    return cfg, off, ads, lens, qoff, qterms, time.time() - t0
+
+
+def split(qoff, qterms, sb):
+    out = []
+    nq = qoff.size - 1
+    for a in range(0, nq, sb):
+        b = min(nq, a + sb)
+        o = (qoff[a:b + 1] - qoff[a]).astype(np.uint64)
+        out.append((a, b, o, qterms[qoff[a]:qoff[b]].astype(np.uint32)))
+    return out
+
+
+def run_ours(args, rank, world, dev):
+    import torch
+    import adabool_b200 as ab
+    from adabool_b200 import Index
+
+    torch.cuda.set_device(dev)
+    cfg, off, ads, lens, qoff, qterms, gen_s = make_workload(args.config, args.scale, args.queries, rank)
+    L = cfg.lists
+    t0 = time.time()
+    ix = Index.from_csr(off, ads, L.n_terms, L.n_ads, device=dev)
+    build_s = time.time() - t0
+    st = ix.stats()
+    n_q = qoff.size - 1
+    n_words = (L.n_ads + 31) // 32
+    stride = (n_words + 3) // 4 * 4
+    path = {"auto": ab.PATH_AUTO, "probe": ab.PATH_PROBE, "union": ab.PATH_UNION, "hybrid": ab.PATH_HYBRID,
+            "tile": ab.PATH_TILE, "planner": ab.PATH_AUTO}[args.path]
+    sbs = split(qoff, qterms, args.sub_batch)
+    max_terms = max(int(s[3].size) for s in sbs) + 1
+    # id capacity: the bound min(n_ads, sum of list lengths) per query
+    qpost = np.add.reduceat(lens[qterms].astype(np.uint64), qoff[:-1].astype(np.int64)) if qterms.size else \
+        np.zeros(n_q, np.uint64)
+    qpost[np.diff(qoff) == 0] = 0
+    bound = np.minimum(qpost, L.n_ads)
+    cap = int(max(bound[a:b].sum() for a, b, _, _ in sbs)) + 1
+    sbq = max(b - a for a, b, _, _ in sbs)
+
+    # device-resident inputs per sub-batch
+    d_in = [(torch.from_numpy(t.view(np.int32)).to(dev) if t.size else torch.zeros(1, dtype=torch.int32, device=dev),
+             torch.from_numpy(o.view(np.int64)).to(dev), b - a) for a, b, o, t in sbs]
+    nbuf = 1 if args.no_e2e else 2
+    ws = [ix.workspace(sbq, max_terms) for _ in range(nbuf)]
+    bms = [torch.empty((sbq, stride), dtype=torch.int32, device=dev) for _ in range(nbuf)]
+    ids = [torch.empty(cap, dtype=torch.int32, device=dev) for _ in range(nbuf)]
+    idoff = [torch.zeros(sbq + 1, dtype=torch.int64, device=dev) for _ in range(nbuf)]
+    stream = torch.cuda.Stream(device=dev)
+
+    def step():
+        for (dt, do, nq) in d_in:
+            ix.batch_run(ws[0], dt, do, nq, bms[0], stride, path=path, d_ids=ids[0], d_id_offsets=idoff[0],
+                         stream=stream)
+
+    # correctness spot check + result sizes (untimed)
+    with torch.cuda.stream(stream):
+        counts = np.zeros(n_q, np.uint64)
+        for (a, b, _, _), (dt, do, nq) in zip(sbs, d_in):
+            ix.batch_run(ws[0], dt, do, nq, bms[0], stride, path=path, d_ids=ids[0], d_id_offsets=idoff[0],
+                         stream=stream)
+            stream.synchronize()
+            o = idoff[0][:nq + 1].cpu().numpy()
+            counts[a:b] = np.diff(o)
+    ws[0].check(stream)
+
+    for _ in range(args.warmup):
+        step()
+    stream.synchronize()
+    dist_barrier(world)
+    ix.profile(True)
+    ix.profile_read()
+    n_launch0 = ab.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    dist_barrier(world)
+    with ClockSampler(dev) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize(dev)
+    launches = (ab.launch_count() - n_launch0) // max(args.steps, 1)
+    ms_total = e0.elapsed_time(e1)
+    kern = ix.profile_read()
+    ix.profile(False)
+    ms_step = dist_max(ms_total / args.steps, world)
+    dist_barrier(world)
+
+    # ---- e2e through the public API from pinned host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, ix, sbs, ws, bms, ids, idoff, stride, path, dev, world, n_q)
+
+    # ---- algorithmic bytes (roofline numerator) ----
+    lbytes = ix.list_bytes().astype(np.float64)
+    hm = ix.tuning.heavy_min_len
+    heavy_t = lens >= (hm if path in (ab.PATH_HYBRID, ab.PATH_AUTO) else (0 if path == ab.PATH_TILE else 1 << 62))
+    qb = lbytes[qterms]
+    q_heavy = np.add.reduceat(np.where(heavy_t[qterms], qb, 0.0), qoff[:-1].astype(np.int64)) if qterms.size else 0
+    q_all = np.add.reduceat(qb, qoff[:-1].astype(np.int64)) if qterms.size else 0
+    empty = np.diff(qoff) == 0
+    q_heavy = np.where(empty, 0.0, q_heavy)
+    q_all = np.where(empty, 0.0, q_all)
+    bm_bytes = L.n_ads / 8.0
+    alg = {
+        "tile_union": float(np.sum(q_heavy)) + n_q * bm_bytes,
+        "scatter_union": float(np.sum(q_all - q_heavy)),
+        "compact_count": n_q * bm_bytes,
+        "compact_write": n_q * bm_bytes + 4.0 * float(counts.sum()),
+    }
+    total_alg = float(np.sum(q_all)) + 16.0 * qterms.size + 2 * n_q * bm_bytes + 4.0 * float(counts.sum())
+    hbm, peak_kind = peaks()
+    per_kernel = {}
+    for name, (nl, tms) in kern.items():
+        per_launch_ms = tms / max(nl, 1)
+        d = {"launches_per_step": nl / args.steps, "ms_per_step": tms / args.steps,
+             "share": tms / max(sum(v[1] for v in kern.values()), 1e-9)}
+        if name in alg and tms > 0:
+            d["achieved_gbs"] = alg[name] * args.steps / (tms / 1e3) / 1e9
+            d["frac_of_" + peak_kind] = d["achieved_gbs"] / hbm
+        per_kernel[name] = d
+    dom = max(per_kernel, key=lambda k: per_kernel[k]["ms_per_step"]) if per_kernel else None
+    roof = None
+    if dom and "achieved_gbs" in per_kernel[dom]:
+        a = per_kernel[dom]["achieved_gbs"]
+        roof = {"kernel": dom, "bound": "hbm", "achieved": round(a, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(a / hbm, 4), "peak_kind": peak_kind, "traffic": None}
+    postings = float(np.sum(qpost))
+    value = n_q * world / (ms_step / 1e3)
+    res = {
+        "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded Zipf lists, lognormal queries)",
+        "config": {"workload": f"{cfg.name}: {L.n_terms} terms x {L.n_ads} ads, {st['n_postings']} postings; "
+                               f"{n_q} queries/rank, sub-batches of {args.sub_batch}",
+                   "path": args.path, "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (no flush)",
+                   "index_bytes": st["device_bytes"], "tuning": ix.tuning.as_dict()},
+        "postings_per_s": round(postings * world / (ms_step / 1e3), 1),
+        "postings_raw_gbs": round(4 * postings * world / (ms_step / 1e3) / 1e9, 1),
+        "algorithmic_gbs": round(total_alg * world / (ms_step / 1e3) / 1e9, 1),
+        "roofline": roof, "kernels": per_kernel, "gpu_launches": int(launches),
+        "result_ids_per_step": int(counts.sum()),
+        "setup_s": {"generate": round(gen_s, 2), "build_upload": round(build_s, 2)},
+    }
+    cs = clk.summary()
+    if cs:
+        res["clocks"] = cs
+    if e2e:
+        res["e2e"] = e2e
+    return res, (off, ads, qoff, qterms, counts)
+
+
+def run_e2e(args, ix, sbs, ws, bms, ids, idoff, stride, path, dev, world, n_q):
+    import torch
+    streams = [torch.cuda.Stream(device=dev) for _ in range(2)]
+    maxt = max(int(t.size) for _, _, _, t in sbs) + 1
+    maxq = max(b - a for a, b, _, _ in sbs) + 1
+    h_terms = [torch.from_numpy(t.view(np.int32) if t.size else np.zeros(1, np.int32)).pin_memory() for _, _, _, t in sbs]
+    h_offs = [torch.from_numpy(o.view(np.int64)).pin_memory() for _, _, o, _ in sbs]
+    d_terms = [torch.empty(maxt, dtype=torch.int32, device=dev) for _ in range(2)]
+    d_offs = [torch.empty(maxq, dtype=torch.int64, device=dev) for _ in range(2)]
+    h_idoff = [torch.empty(maxq, dtype=torch.int64).pin_memory() for _ in range(2)]
+    h_ids = [torch.empty(ids[0].numel(), dtype=torch.int32).pin_memory() for _ in range(2)]
+    ev_off = [torch.cuda.Event() for _ in range(2)]
+    done = [torch.cuda.Event() for _ in range(2)]
+    for e in done:
+        e.record(streams[0])
+    h2d = d2h = 0
+
+    def one_step():
+        nonlocal h2d, d2h
+        h2d = d2h = 0
+        for i, (a, b, o, t) in enumerate(sbs):
+            k = i % 2
+            s = streams[k]
+            nq = b - a
+            done[k].synchronize()  # pinned buffers of set k are free again
+            with torch.cuda.stream(s):
+                d_terms[k][:h_terms[i].numel()].copy_(h_terms[i], non_blocking=True)
+                d_offs[k][:nq + 1].copy_(h_offs[i], non_blocking=True)
+                ix.batch_run(ws[k], d_terms[k], d_offs[k], nq, bms[k], stride, path=path, d_ids=ids[k],
+                             d_id_offsets=idoff[k], stream=s)
+                h_idoff[k][:nq + 1].copy_(idoff[k][:nq + 1], non_blocking=True)
+                ev_off[k].record(s)
+            h2d += t.size * 4 + (nq + 1) * 8
+            ev_off[k].synchronize()
+            tot = int(h_idoff[k][nq])
+            with torch.cuda.stream(s):
+                if tot:
+                    h_ids[k][:tot].copy_(ids[k][:tot], non_blocking=True)
+                done[k].record(s)
+            d2h += (nq + 1) * 8 + tot * 4
+        for s in streams:
+            s.synchronize()
+
+    for _ in range(max(1, min(args.warmup, 2))):
+        one_step()
+    torch.cuda.synchronize(dev)
+    dist_barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(streams[0])
+    streams[1].wait_event(e0)
+    for _ in range(args.steps):
+        one_step()
+    streams[0].wait_stream(streams[1])
+    e1.record(streams[0])
+    e1.synchronize()
+    ms = dist_max(e0.elapsed_time(e1) / args.steps, world)
+    return {"value": round(n_q * world / (ms / 1e3), 2), "unit": UNIT, "ms_per_step": round(ms, 3),
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "note": "query terms host->device and every sorted id list device->host, pinned buffers, 2 streams"}
+
+
+def cpu_baseline(off, ads, qoff, qterms, seconds: float):
+    """Oracle k-way merge (a port of the match-set semantics) on all host cores."""
+    from oracle import oracle as O
+    n_threads = os.cpu_count() or 1
+    lens = np.diff(off)
+    # single-core rate on the first query with work
+    i0 = int(np.argmax(np.diff(qoff) > 0))
+    t0 = time.time()
+    O.cpu_batch(off, ads, qoff[i0:i0 + 2] - qoff[i0], qterms[qoff[i0]:qoff[i0 + 1]], 1)
+    one = max(time.time() - t0, 1e-6)
+    post0 = float(lens[qterms[qoff[i0]:qoff[i0 + 1]]].sum())
+    rate = post0 / one  # postings per second per core
+    qpost = np.array([lens[qterms[qoff[i]:qoff[i + 1]]].sum() for i in range(qoff.size - 1)], np.float64)
+    budget = rate * seconds * n_threads
+    m = int(np.searchsorted(np.cumsum(qpost), budget)) + 1
+    m = max(min(m, qoff.size - 1), min(n_threads, qoff.size - 1))
+    t0 = time.time()
+    O.cpu_batch(off, ads, qoff[:m + 1], qterms[:qoff[m]], n_threads)
+    dt = time.time() - t0
+    return {"value": round(m / dt, 3), "unit": UNIT, "cores": n_threads, "kind": "port",
+            "sample": f"first {m} queries of the same set ({qpost[:m].sum():.3g} postings), heap k-way merge "
+                      f"to sorted ids, {n_threads} threads, {dt:.1f} s",
+            "single_core_value": round(1.0 / one, 3), "single_core_sample": f"query {i0} ({post0:.3g} postings)"}
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args):
+    """The reference's CPU path on the host cores (bounded sample)."""
+    from oracle import oracle as O
+    from adabool_b200 import workload as W
+    cfg, off, ads, lens, qoff, qterms, _ = make_workload(args.config, args.scale, args.queries, 0)
+    n_threads = os.cpu_count() or 1
+    H = O.ref_harness_lib()
+    qpost = np.array([lens[qterms[qoff[i]:qoff[i + 1]]].sum() for i in range(qoff.size - 1)], np.float64)
+    if H is not None:
+        terms, ads_c = W.lists_to_coo(off, ads)
+        h = H.refq_cpu_load(O._p(np.ascontiguousarray(terms), O.u32p), O._p(ads_c, O.u32p), terms.size)
+        kind = "reference"
+        desc = "ComputeGroundTruth (reference CPU path, std::set over every COO pair)"
+
+        def run(m):
+            counts = np.zeros(m, np.uint64)
+            H.refq_ground_truth_batch(h, O._p(np.ascontiguousarray(qoff[:m + 1]), O.u64p),
+                                      O._p(np.ascontiguousarray(qterms[:qoff[m]]), O.u32p), m, n_threads,
+                                      O._p(counts, O.u64p))
+    else:
+        kind = "port"
+        desc = "oracle heap k-way merge (reference library not built)"
+
+        def run(m):
+            O.cpu_batch(off, ads, qoff[:m + 1], qterms[:qoff[m]], n_threads)
+    # the reference's scan costs the same per query whatever its size: one
+    # query per thread per step keeps a step to a few seconds
+    m = min(n_threads, qoff.size - 1) if kind == "reference" else max(1, min(qoff.size - 1, n_threads))
+    for _ in range(args.warmup):
+        run(min(m, n_threads))
+    times = []
+    for _ in range(args.steps):
+        t0 = time.time()
+        run(m)
+        times.append(time.time() - t0)
+    sec = float(np.mean(times))
+    v = m / sec
+    sample = f"{desc}: first {m} queries of {cfg.name} per step ({qpost[:m].sum():.3g} postings), {n_threads} threads"
+    return {"impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(sec * 1e3, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": f"{cfg.name}: {cfg.lists.n_terms} terms x {cfg.lists.n_ads} ads, "
+                                   f"{int(off[-1])} postings", "parallelism": "host threads"},
+            "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": n_threads, "kind": kind, "sample": sample},
+            "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+# ---------------------------------------------------------------------------
+_PG = None
+
+
+def dist_init(args):
+    global _PG
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        _PG = dist
+    return rank, world, local
+
+
+def dist_barrier(world):
+    if world > 1 and _PG is not None:
+        _PG.barrier()
+
+
+def dist_max(x: float, world: int) -> float:
+    if world > 1 and _PG is not None:
+        import torch
+        dev = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        _PG.all_reduce(t, op=_PG.ReduceOp.MAX)
+        return float(t.item())
+    return x
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return 0
+        res = run_reference(args)
+    else:
+        rank, world, local = dist_init(args)
+        res, data = run_ours(args, rank, world, local)
+        if rank == 0 and not args.no_cpu:
+            off, ads, qoff, qterms, _ = data
+            res["cpu_baseline"] = cpu_baseline(off, ads, qoff, qterms, args.cpu_seconds)
+        if _PG is not None:
+            _PG.destroy_process_group()
+        if rank != 0:
+            return 0
+    line = json.dumps(res)
+    print(line, flush=True)
+    if args.out:
+        with open(args.out, "a") as f:
+            f.write(line + "\n")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,292 @@
+/*
+ * adabool.h -- C ABI of the B200 Boolean-filtering engine (libadabool.so).
+ *
+ * A filter matrix is a set of (term, ad) pairs. A query is a set of terms;
+ * its match set is the OR-union of the posting lists of its terms, returned
+ * as a bitmap over ads (word v>>5, bit v&31 -- the layout the reference's
+ * kernels write and CollectIdsFromBitmap reads, test/adsfilter_batch.cu:82-97)
+ * and, optionally, as an ascending list of uint32 ad IDs.
+ *
+ * Conventions (all entry points):
+ *   - every function returns abf_status; nothing aborts and no C++ exception
+ *     crosses this boundary; abf_last_error_string() describes the last
+ *     failure on the calling thread;
+ *   - pointers named d_* are device pointers on the index's device; h_*
+ *     and plain pointers are host pointers;
+ *   - stream arguments are cudaStream_t passed as void* (0 = legacy default);
+ *     all device work is enqueued on that stream and the call returns
+ *     without synchronising unless its comment says otherwise;
+ *   - an index or worker is used by one stream at a time (the reference has
+ *     the same rule: one caller stream, no internal locks).
+ *
+ * Each entry point names the reference interface it replaces as
+ * file:line within the reference project (yxr620/AdaBool).
+ */
+#ifndef ADABOOL_H_
+#define ADABOOL_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ABF_ABI_VERSION 1u
+/* postings per compressed block of the list format */
+#define ABF_BLOCK_POSTINGS 128u
+
+typedef enum abf_status {
+    ABF_OK = 0,
+    ABF_ERR_INVALID = 1,   /* bad argument (null pointer, zero size, ...) */
+    ABF_ERR_RANGE = 2,     /* a term or ad id outside the declared domain */
+    ABF_ERR_CUDA = 3,      /* a CUDA runtime call failed */
+    ABF_ERR_OOM = 4,       /* host or device allocation failed */
+    ABF_ERR_STATE = 5,     /* object not in a state that allows the call */
+    ABF_ERR_IO = 6,        /* file read/write failed or bad file format */
+    ABF_ERR_TIMEOUT = 7,   /* a bounded device-side wait gave up */
+    ABF_ERR_CAPACITY = 8,  /* output larger than the capacity given */
+    ABF_ERR_INTERNAL = 9
+} abf_status;
+
+/* Which kernel family answers a query. */
+typedef enum abf_path {
+    ABF_PATH_AUTO = 0,    /* planner decides per query (learned, else fixed rule) */
+    ABF_PATH_PROBE = 1,   /* bitmap-probe: scan every block, test the query's term bitmap */
+    ABF_PATH_UNION = 2,   /* list-union: decode only the query's lists, scatter to the bitmap */
+    ABF_PATH_HYBRID = 3,  /* long lists merged tile by tile in shared memory, short lists scattered */
+    ABF_PATH_TILE = 4     /* every list merged tile by tile (HYBRID with threshold 0) */
+} abf_path;
+
+typedef struct abf_index abf_index;
+typedef struct abf_workspace abf_workspace;
+typedef struct abf_worker abf_worker;
+
+/* ------------------------------------------------------------------ */
+/* Index build / free / persistence                                    */
+/* ------------------------------------------------------------------ */
+
+enum {
+    ABF_BUILD_HOST_ONLY = 1u << 0, /* keep the index on the host; no device needed */
+    ABF_BUILD_KEEP_HOST = 1u << 1  /* keep a host copy after the upload */
+};
+
+typedef struct abf_build_opts {
+    int device;          /* CUDA device ordinal (ignored with ABF_BUILD_HOST_ONLY) */
+    uint32_t flags;      /* ABF_BUILD_* */
+    int n_threads;       /* host threads for the build; <= 0 = all cores */
+} abf_build_opts;
+
+typedef struct abf_index_stats {
+    uint32_t n_terms;
+    uint32_t n_ads;
+    uint64_t n_postings;        /* unique (term, ad) pairs */
+    uint64_t n_blocks;          /* compressed blocks */
+    uint64_t payload_bytes;     /* bit-packed gap bytes */
+    uint64_t device_bytes;      /* all device arrays of the index */
+    uint32_t max_list_len;
+    uint32_t on_device;         /* 1 if the device copy exists */
+} abf_index_stats;
+
+/* Build from COO pairs (terms[i], ads[i]), i < nnz. Pairs may be in any
+ * order; duplicates are merged. Every term must be < n_terms and every ad
+ * < n_ads, else ABF_ERR_RANGE. Replaces ivf_list::BuildFrom
+ * (src/AdaBool/inverted_list.h:348-374) and the per-block key metadata it
+ * derives (src/AdaBool/inverted_list.h:90-148). */
+abf_status abf_index_build_coo(const uint32_t* terms, const uint32_t* ads, uint64_t nnz,
+                               uint32_t n_terms, uint32_t n_ads,
+                               const abf_build_opts* opts, abf_index** out);
+
+/* Build from CSR: the postings of term t are ads[offsets[t] .. offsets[t+1]),
+ * offsets has n_terms+1 entries. Lists need not be sorted or unique. Same
+ * replacement as abf_index_build_coo, without the COO grouping step
+ * (src/AdaBool/inverted_list.h:351-355). */
+abf_status abf_index_build_csr(const uint64_t* offsets, const uint32_t* ads,
+                               uint32_t n_terms, uint32_t n_ads,
+                               const abf_build_opts* opts, abf_index** out);
+
+/* Frees the index and its device arrays (synchronises the device). The
+ * reference frees through LenBuffer destructors (src/AdaBool/len_buffer.h:196-230). */
+abf_status abf_index_free(abf_index* index);
+
+abf_status abf_index_get_stats(const abf_index* index, abf_index_stats* out);
+
+/* Per-term list lengths (n_terms entries) into a host array. */
+abf_status abf_index_list_lengths(const abf_index* index, uint32_t* h_out, uint32_t n);
+
+/* Decode the list of one term on the host from the compressed arrays
+ * (needs the host copy: ABF_BUILD_HOST_ONLY or ABF_BUILD_KEEP_HOST).
+ * *n_out receives the list length; at most cap ids are written. */
+abf_status abf_index_decode_list(const abf_index* index, uint32_t term,
+                                 uint32_t* h_ids, uint64_t cap, uint64_t* n_out);
+
+/* Binary index file: one header plus the compressed arrays, loaded with a
+ * single host read and one upload per array. No reference counterpart: the
+ * reference rebuilds from text COO on every run (test/adsfilter_q_all.cu:127-161). */
+abf_status abf_index_save(const abf_index* index, const char* path);
+abf_status abf_index_load(const char* path, const abf_build_opts* opts, abf_index** out);
+
+/* Upload a host-only index to a device. */
+abf_status abf_index_to_device(abf_index* index, int device);
+
+/* ------------------------------------------------------------------ */
+/* Kernel tuning                                                       */
+/* ------------------------------------------------------------------ */
+
+typedef struct abf_tuning {
+    uint32_t tile_words;      /* words per merge tile: 256, 512 or 1024 */
+    uint32_t warps_per_tile;  /* warps that share one tile's lists: 1, 2, 4 or 8 */
+    uint32_t heavy_min_len;   /* HYBRID: lists with >= this many postings are merged
+                                 per tile, shorter lists are scattered */
+    uint32_t probe_chunk_blocks; /* blocks per CTA in the bitmap-probe scan */
+    uint32_t scatter_blocks_per_warp; /* consecutive blocks a union warp takes */
+    uint32_t ctas_per_sm;     /* grid = SMs x this, for the persistent kernels */
+    uint32_t probe_cap;       /* queries of one batch that may take the probe path */
+    float probe_min_fraction; /* fixed rule (ABF_PATH_AUTO without a planner): probe
+                                 when the query's lists hold more than this fraction
+                                 of all blocks, else list-union */
+} abf_tuning;
+
+abf_status abf_get_tuning(const abf_index* index, abf_tuning* out);
+abf_status abf_set_tuning(abf_index* index, const abf_tuning* t);
+
+/* ------------------------------------------------------------------ */
+/* Reference-shaped operator API (prepare a worker, run it into d_res)  */
+/* ------------------------------------------------------------------ */
+/* These keep the reference's contract: d_res is caller-owned and the
+ * kernels OR into it, so a caller that zeroes d_res gets exactly the match
+ * set; the bitmap has (n_ads + 31) / 32 words per query. */
+
+/* Sparse worker for one query (or a flattened batch of queries) given as
+ * host term ids; terms >= n_terms are ignored. Replaces
+ * ivf_list::Prepare(keys) (src/AdaBool/inverted_list.h:481-527) together
+ * with InvertedListWorker::Prepare / LoadBalanceTransformer::Prepare
+ * (src/AdaBool/inverted_list.h:183-189, src/AdaBool/load_balance_transformer.h:50-69). */
+abf_status abf_prepare_sparse(abf_index* index, const uint32_t* keys, uint64_t n_keys,
+                              abf_worker** out);
+
+/* Dense worker for one query given as a host term bitmap of len bytes
+ * (bit t of byte t/8 set = term t in the query). Replaces
+ * ivf_list::Prepare(len, bitmap) (src/AdaBool/inverted_list.h:530-543). */
+abf_status abf_prepare_dense(abf_index* index, uint64_t len, const uint8_t* query_bitmap,
+                             abf_worker** out);
+
+/* Dense worker for batch_size queries whose term bitmaps are laid out
+ * query-major, len bytes each (len a multiple of 4). Host variant replaces
+ * ivf_list::PrepareBatch (src/AdaBool/inverted_list.h:564-574); the device
+ * variant replaces PrepareBatchDevice (src/AdaBool/inverted_list.h:591-605)
+ * and does not copy d_query_bitmap, which must outlive the worker. */
+abf_status abf_prepare_batch(abf_index* index, uint64_t batch_size, uint64_t len,
+                             const uint8_t* query_bitmap, abf_worker** out);
+abf_status abf_prepare_batch_device(abf_index* index, uint64_t batch_size, uint64_t len,
+                                    const uint8_t* d_query_bitmap, abf_worker** out);
+
+abf_status abf_worker_free(abf_worker* worker);
+
+/* Union of the sparse worker's lists ORed into d_res. Replaces
+ * ListUnion_sparse (test/adsfilter_q_all.cu:64-105). */
+abf_status abf_list_union_sparse(const abf_worker* worker, uint32_t* d_res, void* stream);
+
+/* Bitmap-probe of the dense worker ORed into d_res. Replaces
+ * ListUnion_dense (test/adsfilter_q_all.cu:26-61). */
+abf_status abf_list_union_dense(const abf_worker* worker, uint32_t* d_res, void* stream);
+
+/* Batched bitmap-probe: query b ORs into d_res + b * res_len_u32. Any batch
+ * size (the reference stops at 32). Replaces BatchListUnion_dense
+ * (test/adsfilter_batch.cu:28-36) and InvertedListBatchWorkerImpl::RunArrays
+ * (src/AdaBool/inverted_list.cu.h:224-228). */
+abf_status abf_batch_list_union_dense(const abf_worker* worker, uint32_t* d_res,
+                                      uint32_t res_len_u32, void* stream);
+
+/* Batched list-union: key i of the sparse worker ORs into
+ * d_res + d_qidx[i] * (res_len_bytes / 4). Replaces BatchListUnion_sparse
+ * (test/adsfilter_batch.cu:39-79). */
+abf_status abf_batch_list_union_sparse(const abf_worker* worker, uint32_t* d_res,
+                                       const uint32_t* d_qidx, uint32_t res_len_bytes,
+                                       void* stream);
+
+/* Ascending ids of the set bits below n_bits of a device bitmap, written
+ * to d_ids (at most ids_capacity), the count to *d_count (device). Replaces
+ * the host-side CollectIdsFromBitmap (test/adsfilter_q_all.cu:108-119,
+ * test/adsfilter_batch.cu:82-97). Uses a workspace of the index. */
+abf_status abf_collect_ids(abf_index* index, const uint32_t* d_bitmap, uint64_t n_bits,
+                           uint32_t* d_ids, uint64_t ids_capacity, uint64_t* d_count,
+                           void* stream);
+
+/* ------------------------------------------------------------------ */
+/* Native batched API (no reference counterpart beyond the batch paths) */
+/* ------------------------------------------------------------------ */
+
+/* A workspace holds the scratch arrays of one in-flight batch: planning
+ * tables, probe bitmaps, compaction counts, an error flag. Sized for at
+ * most max_queries queries and max_terms query terms in total. */
+abf_status abf_workspace_create(abf_index* index, uint32_t max_queries, uint64_t max_terms,
+                                abf_workspace** out);
+abf_status abf_workspace_free(abf_workspace* ws);
+/* Reads and clears the device error flag (synchronises the stream). */
+abf_status abf_workspace_check(abf_workspace* ws, void* stream);
+
+typedef struct abf_batch {
+    const uint32_t* d_terms;     /* flat query terms (device) */
+    const uint64_t* d_offsets;   /* n_queries + 1 offsets into d_terms (device) */
+    uint32_t n_queries;
+    const uint8_t* d_paths;      /* per-query abf_path (device) or NULL */
+    abf_path path;               /* used when d_paths is NULL; AUTO = fixed rule per query */
+    uint32_t* d_bitmaps;         /* n_queries x bitmap_stride_words output bitmaps, overwritten */
+    uint64_t bitmap_stride_words;/* >= (n_ads + 31) / 32, a multiple of 4 */
+    uint32_t* d_ids;             /* optional: packed ascending ids of every query */
+    uint64_t ids_capacity;       /* entries available in d_ids */
+    uint64_t* d_id_offsets;      /* optional (required with d_ids): n_queries + 1 */
+} abf_batch;
+
+/* Runs a batch: planning, merge tiles, scatter, probe and (with d_ids)
+ * compaction, all on `stream`, no host synchronisation and no allocation,
+ * so the call can be captured into a CUDA graph. Queries whose ids do not
+ * fit ids_capacity get their offsets but ids are written only below the
+ * capacity. */
+abf_status abf_batch_run(abf_index* index, abf_workspace* ws, const abf_batch* batch,
+                         void* stream);
+
+/* One query from host terms: bitmap (overwritten, (n_ads+31)/32 words) and,
+ * if d_ids is not NULL, its ascending ids with the count in *d_count. Uses
+ * the index's own workspace; the call returns after the terms were
+ * uploaded, without waiting for the kernels. */
+abf_status abf_query(abf_index* index, const uint32_t* terms, uint32_t n_terms, abf_path path,
+                     uint32_t* d_bitmap, uint32_t* d_ids, uint64_t ids_capacity,
+                     uint64_t* d_count, void* stream);
+
+/* ------------------------------------------------------------------ */
+/* Measurement                                                         */
+/* ------------------------------------------------------------------ */
+
+/* Compressed bytes of every term's list (n_terms entries): payload plus
+ * 16 bytes of block metadata per block. No reference counterpart. */
+abf_status abf_index_list_bytes(const abf_index* index, uint64_t* h_out, uint32_t n);
+
+/* Kernel timing. While enabled, every kernel this index launches is
+ * bracketed by CUDA events on the stream it is launched on;
+ * abf_profile_read synchronises those events, returns per-kernel launch
+ * counts and total milliseconds, and clears them. No reference counterpart
+ * (the reference times launch + synchronise with a host clock,
+ * test/adsfilter_q_all.cu:421-425). */
+typedef struct abf_kernel_time {
+    char name[24];
+    uint64_t launches;
+    double total_ms;
+} abf_kernel_time;
+abf_status abf_profile_enable(abf_index* index, int on);
+abf_status abf_profile_read(abf_index* index, abf_kernel_time* out, uint32_t cap, uint32_t* n_out);
+
+/* ------------------------------------------------------------------ */
+/* Misc                                                                */
+/* ------------------------------------------------------------------ */
+const char* abf_last_error_string(void);
+const char* abf_status_string(abf_status s);
+uint32_t abf_abi_version(void);
+/* Number of kernel launches this library has enqueued since load. */
+uint64_t abf_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ADABOOL_H_ */
