@@ -33,13 +33,17 @@ QCOUNT_LOGNORMAL = 1
 
 
 class BuildOpts(C.Structure):
-    _fields_ = [("device", C.c_int), ("flags", C.c_uint32), ("n_threads", C.c_int)]
+    _fields_ = [("device", C.c_int), ("flags", C.c_uint32), ("n_threads", C.c_int), ("dense_div", C.c_uint32)]
+
+
+DENSE_NONE = 0xFFFFFFFF
 
 
 class IndexStats(C.Structure):
     _fields_ = [("n_terms", C.c_uint32), ("n_ads", C.c_uint32), ("n_postings", C.c_uint64),
                 ("n_blocks", C.c_uint64), ("payload_bytes", C.c_uint64), ("device_bytes", C.c_uint64),
-                ("max_list_len", C.c_uint32), ("on_device", C.c_uint32)]
+                ("max_list_len", C.c_uint32), ("on_device", C.c_uint32), ("n_dense_lists", C.c_uint32),
+                ("n_directory_lists", C.c_uint32), ("dense_bytes", C.c_uint64)]
 
 
 class Tuning(C.Structure):
@@ -102,6 +106,7 @@ PROTOTYPES = {
     "abf_batch_run": [vp, vp, C.POINTER(Batch), vp],
     "abf_query": [vp, u32p, C.c_uint32, C.c_int, vp, vp, C.c_uint64, vp, vp],
     "abf_index_list_bytes": [vp, u64p, C.c_uint32],
+    "abf_index_list_flags": [vp, u32p, C.c_uint32],
     "abf_profile_enable": [vp, C.c_int],
     "abf_profile_read": [vp, vp, C.c_uint32, u32p],
     "abf_last_error_string": [],

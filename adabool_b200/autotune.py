@@ -1,0 +1,126 @@
+"""Autotuner for the batch kernels.
+
+Times abf_batch_run (CUDA events on the launching stream) on a sample of
+the caller's queries for candidate values of each knob -- merge tile width,
+warps sharing a tile, the merge/scatter switch length (the dense/sparse
+switch point of the hybrid path), CTAs per SM, blocks per scatter warp --
+and keeps the fastest, one knob at a time (coordinate descent, a few
+rounds). Results are bit-exact whatever the knobs; only time changes. The
+outcome can be written to a JSON file and applied to a later index with
+``apply``.
+
+The reference fixes these at compile time (kKeyStep = 256, kThreadNum = 64,
+test/adsfilter_q_all.cu:22-23) and has no tuner.
+"""
+from __future__ import annotations
+
+import json
+import time
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+from . import _native as N
+
+KNOBS = {
+    "tile_words": [256, 512, 1024, 2048, 4096, 8192, 16384],
+    "warps_per_tile": [1, 2, 4, 8],
+    "ctas_per_sm": [2, 4, 6, 8],
+    "scatter_blocks_per_warp": [1, 2, 4, 8],
+}
+
+
+def heavy_candidates(n_ads: int) -> list[int]:
+    """Merge/scatter switch lengths: lists holding 1/4096 .. 1/16 of the ads."""
+    return sorted({max(128, n_ads // d) for d in (4096, 1024, 512, 256, 128, 64, 32, 16)})
+
+
+@dataclass
+class TuneResult:
+    best: dict
+    best_ms: float
+    trials: list = field(default_factory=list)
+
+    def save(self, path):
+        Path(path).write_text(json.dumps({"best": self.best, "best_ms": self.best_ms, "trials": self.trials},
+                                         indent=1))
+
+
+def apply(index, path_or_dict):
+    d = path_or_dict if isinstance(path_or_dict, dict) else json.loads(Path(path_or_dict).read_text())["best"]
+    index.set_tuning(**{k: v for k, v in d.items() if k in dict(N.Tuning._fields_)})
+
+
+class _Runner:
+    def __init__(self, index, q_off, q_terms, sub_batch, path, device):
+        import torch
+        self.torch = torch
+        self.ix = index
+        self.path = path
+        n_q = q_off.size - 1
+        self.stride = (index.n_words + 3) // 4 * 4
+        self.sbs = []
+        for a in range(0, n_q, sub_batch):
+            b = min(n_q, a + sub_batch)
+            o = (q_off[a:b + 1] - q_off[a]).astype(np.uint64)
+            t = q_terms[q_off[a]:q_off[b]].astype(np.uint32)
+            dt = torch.from_numpy(t.view(np.int32)).to(device) if t.size else torch.zeros(1, dtype=torch.int32,
+                                                                                          device=device)
+            self.sbs.append((dt, torch.from_numpy(o.view(np.int64)).to(device), b - a))
+        mq = max(s[2] for s in self.sbs)
+        mt = max(int(s[0].numel()) for s in self.sbs) + 1
+        self.ws = index.workspace(mq, mt)
+        self.bms = torch.empty((mq, self.stride), dtype=torch.int32, device=device)
+        self.stream = torch.cuda.Stream(device=device)
+
+    def time_ms(self, reps: int) -> float:
+        torch = self.torch
+        for dt, do, nq in self.sbs:  # warm-up (also rebuilds nothing: tuning is read per launch)
+            self.ix.batch_run(self.ws, dt, do, nq, self.bms, self.stride, path=self.path, stream=self.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(self.stream)
+        for _ in range(reps):
+            for dt, do, nq in self.sbs:
+                self.ix.batch_run(self.ws, dt, do, nq, self.bms, self.stride, path=self.path, stream=self.stream)
+        e1.record(self.stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+
+def autotune(index, q_off: np.ndarray, q_terms: np.ndarray, path: int = N.PATH_HYBRID, sub_batch: int = 64,
+             sample: int = 512, reps: int = 2, rounds: int = 2, knobs: dict | None = None, device: int = 0,
+             verbose: bool = False) -> TuneResult:
+    """Coordinate-descent tuning on the first `sample` queries; leaves the
+    best tuning set on the index and returns it with every trial."""
+    n = min(sample, q_off.size - 1)
+    run = _Runner(index, q_off[:n + 1], q_terms[:q_off[n]], sub_batch, path, device)
+    space = dict(KNOBS if knobs is None else knobs)
+    space.setdefault("heavy_min_len", heavy_candidates(index.n_ads))
+    cur = index.tuning.as_dict()
+    trials = []
+    best_ms = run.time_ms(reps)
+    trials.append({"tuning": dict(cur), "ms": best_ms})
+    for _ in range(rounds):
+        improved = False
+        for knob, values in space.items():
+            for v in values:
+                if cur.get(knob) == v:
+                    continue
+                cand = dict(cur)
+                cand[knob] = v
+                try:
+                    index.set_tuning(**{knob: v})
+                except N.AbfError:
+                    continue
+                ms = run.time_ms(reps)
+                trials.append({"tuning": cand, "ms": ms})
+                if verbose:
+                    print(f"  {knob}={v}: {ms:.3f} ms (best {best_ms:.3f})", flush=True)
+                if ms < best_ms * 0.995:
+                    best_ms, cur, improved = ms, cand, True
+                index.set_tuning(**{k: cur[k] for k in space})
+        if not improved:
+            break
+    index.set_tuning(**{k: cur[k] for k in space})
+    return TuneResult(best={k: cur[k] for k in cur}, best_ms=best_ms, trials=trials)

@@ -271,6 +271,66 @@ void decode_block_host(const HostIndex& h, uint64_t b, uint32_t* out) {
     }
 }
 
+void derive_tables(const HostIndex& h, uint32_t dense_div, int n_threads, DerivedHost* out) {
+    n_threads = resolve_threads(n_threads);
+    const uint64_t n_words = (uint64_t(h.n_ads) + 31) / 32;
+    out->dense_stride = (n_words + 3) & ~uint64_t(3);
+    out->term_dense.assign(h.n_terms, kNone);
+    out->term_dir.assign(h.n_terms, kNone);
+    out->dir_n = uint32_t(((uint64_t(h.n_ads) + (1u << kDirShift) - 1) >> kDirShift) + 1);
+    if (dense_div == 0) dense_div = kDefaultDenseDiv;
+    // dense candidates, longest first, within a memory budget of twice the
+    // payload (at least 256 MB)
+    std::vector<uint32_t> cand;
+    for (uint32_t t = 0; t < h.n_terms; ++t)
+        if (dense_div != kNone && h.term_len[t] && uint64_t(h.term_len[t]) * dense_div >= h.n_ads) cand.push_back(t);
+    std::sort(cand.begin(), cand.end(), [&](uint32_t a, uint32_t b) { return h.term_len[a] > h.term_len[b]; });
+    const uint64_t budget = std::max<uint64_t>(256ull << 20, 2ull * 16ull * h.payload.size());
+    std::vector<uint32_t> dense_terms;
+    for (uint32_t t : cand) {
+        if ((dense_terms.size() + 1) * out->dense_stride * 4 > budget) break;
+        out->term_dense[t] = uint32_t(dense_terms.size());
+        dense_terms.push_back(t);
+    }
+    out->n_dense = uint32_t(dense_terms.size());
+    std::vector<uint32_t> dir_terms;
+    for (uint32_t t = 0; t < h.n_terms; ++t) {
+        if (out->term_dense[t] != kNone) continue;
+        if (uint64_t(h.term_len[t]) * kDirDiv >= h.n_ads && h.term_blk[t + 1] - h.term_blk[t] >= 2) {
+            out->term_dir[t] = uint32_t(dir_terms.size()) * out->dir_n;
+            dir_terms.push_back(t);
+        }
+    }
+    out->n_dir = uint32_t(dir_terms.size());
+    out->dense.assign(size_t(out->n_dense) * out->dense_stride, 0u);
+    out->dir.assign(size_t(out->n_dir) * out->dir_n, 0u);
+    parallel_for(n_threads, out->n_dense, [&](int, uint64_t b, uint64_t e) {
+        uint32_t buf[kBlock];
+        for (uint64_t i = b; i < e; ++i) {
+            const uint32_t t = dense_terms[i];
+            uint32_t* bm = out->dense.data() + i * out->dense_stride;
+            for (uint32_t blk = h.term_blk[t]; blk < h.term_blk[t + 1]; ++blk) {
+                decode_block_host(h, blk, buf);
+                const uint32_t cnt = desc_count(h.blk_desc[blk].y);
+                for (uint32_t k = 0; k < cnt; ++k) bm[buf[k] >> 5] |= 1u << (buf[k] & 31u);
+            }
+        }
+    });
+    parallel_for(n_threads, out->n_dir, [&](int, uint64_t b, uint64_t e) {
+        for (uint64_t i = b; i < e; ++i) {
+            const uint32_t t = dir_terms[i];
+            uint32_t* d = out->dir.data() + i * out->dir_n;
+            uint32_t blk = h.term_blk[t];
+            const uint32_t b1 = h.term_blk[t + 1];
+            for (uint32_t j = 0; j < out->dir_n; ++j) {
+                const uint64_t lo = uint64_t(j) << kDirShift;
+                while (blk < b1 && uint64_t(h.blk_last[blk]) < lo) ++blk;
+                d[j] = blk;
+            }
+        }
+    });
+}
+
 }  // namespace abf
 
 // ---------------------------------------------------------------------------

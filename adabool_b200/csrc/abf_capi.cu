@@ -126,6 +126,7 @@ struct abf_workspace {
     uint32_t chunks_per_q = 0;
     uint32_t* heavy = nullptr;
     uint32_t* lpref = nullptr;
+    uint32_t* tile_cls = nullptr;
     uint64_t* lcnt = nullptr;
     uint64_t* lpref_q = nullptr;
     uint32_t* probe_list = nullptr;
@@ -152,6 +153,7 @@ struct abf_worker {
     uint64_t* d_offk = nullptr;     // 0..n_keys: every key its own query
     uint32_t* d_heavy = nullptr;
     uint32_t* d_lpref = nullptr;
+    uint32_t* d_tile_cls = nullptr;
     uint64_t* d_lcnt = nullptr;
     uint64_t* d_lpref_q = nullptr;
     uint32_t* d_nprobe = nullptr;
@@ -204,14 +206,14 @@ void default_tuning(abf_index* ix) {
     abf_tuning& t = ix->tuning;
     t.tile_words = 1024;
     t.warps_per_tile = 8;
-    // a list is merged per tile when its blocks are on average no wider than
-    // one tile (128 ids per block spread over n_ads / len ids)
-    uint64_t span = uint64_t(t.tile_words) * 32u;
-    uint64_t m = (uint64_t(abf::kBlock) * ix->n_ads + span - 1) / span;
-    t.heavy_min_len = uint32_t(std::max<uint64_t>(m, abf::kBlock));
+    // HYBRID merges per tile the lists holding at least 1/32 of the ads (the
+    // ones that also get dense bitmaps); measured on the 2^24-ad workload,
+    // decoding shorter lists inside the tiles loses to scattering them, as a
+    // tile holds only a block or two of each
+    t.heavy_min_len = uint32_t(std::max<uint64_t>((uint64_t(ix->n_ads) + 31) / 32, abf::kBlock));
     t.probe_chunk_blocks = 256;
-    t.scatter_blocks_per_warp = 4;
-    t.ctas_per_sm = 2;
+    t.scatter_blocks_per_warp = 8;
+    t.ctas_per_sm = 6;
     t.probe_cap = 32;
     t.probe_min_fraction = 0.5f;
 }
@@ -225,6 +227,10 @@ void free_device(abf_index* ix) {
     dev_free(d.blk_term);
     dev_free(d.blk_desc);
     dev_free(d.payload);
+    dev_free(d.term_dense);
+    dev_free(d.dense);
+    dev_free(d.term_dir);
+    dev_free(d.dir);
     d.bytes = 0;
     ix->on_device = false;
 }
@@ -245,7 +251,11 @@ abf_status upload(abf_index* ix, int device) {
         (st = upload_vec(&d.blk_last, h.blk_last, &d.bytes)) != ABF_OK ||
         (st = upload_vec(&d.blk_term, h.blk_term, &d.bytes)) != ABF_OK ||
         (st = upload_vec(&d.blk_desc, h.blk_desc, &d.bytes)) != ABF_OK ||
-        (st = upload_vec(&d.payload, h.payload, &d.bytes)) != ABF_OK) {
+        (st = upload_vec(&d.payload, h.payload, &d.bytes)) != ABF_OK ||
+        (st = upload_vec(&d.term_dense, ix->derived.term_dense, &d.bytes)) != ABF_OK ||
+        (st = upload_vec(&d.dense, ix->derived.dense, &d.bytes)) != ABF_OK ||
+        (st = upload_vec(&d.term_dir, ix->derived.term_dir, &d.bytes)) != ABF_OK ||
+        (st = upload_vec(&d.dir, ix->derived.dir, &d.bytes)) != ABF_OK) {
         free_device(ix);
         return st;
     }
@@ -273,6 +283,8 @@ abf_status finalize(abf_index* ix, const abf_build_opts* opts) {
         ix->h_term_bytes[t] = bytes;
     }
     ix->host_valid = true;
+    ix->dense_div = (opts && opts->dense_div) ? opts->dense_div : abf::kDefaultDenseDiv;
+    abf::derive_tables(h, ix->dense_div, opts ? opts->n_threads : 0, &ix->derived);
     default_tuning(ix);
     uint32_t flags = opts ? opts->flags : 0u;
     if (!(flags & ABF_BUILD_HOST_ONLY)) {
@@ -280,6 +292,9 @@ abf_status finalize(abf_index* ix, const abf_build_opts* opts) {
         if (!(flags & ABF_BUILD_KEEP_HOST)) {
             ix->host = abf::HostIndex();
             ix->host_valid = false;
+            // keep the small per-term tables, drop the bitmaps and directory
+            ix->derived.dense = std::vector<uint32_t>();
+            ix->derived.dir = std::vector<uint32_t>();
         }
     }
     return ABF_OK;
@@ -294,6 +309,7 @@ abf_status need_device(const abf_index* ix) {
 void ws_release(abf_workspace* w) {
     dev_free(w->heavy);
     dev_free(w->lpref);
+    dev_free(w->tile_cls);
     dev_free(w->lcnt);
     dev_free(w->lpref_q);
     dev_free(w->probe_list);
@@ -320,6 +336,7 @@ abf_status ws_alloc(abf_index* ix, uint32_t max_q, uint64_t max_terms, uint64_t 
     const uint64_t chunks = uint64_t(max_q) * w->chunks_per_q;
     abf_status st;
     if ((st = dev_alloc(&w->heavy, max_q)) != ABF_OK || (st = dev_alloc(&w->lpref, max_terms)) != ABF_OK ||
+        (st = dev_alloc(&w->tile_cls, max_terms)) != ABF_OK ||
         (st = dev_alloc(&w->lcnt, max_q)) != ABF_OK || (st = dev_alloc(&w->lpref_q, uint64_t(max_q) + 1)) != ABF_OK ||
         (st = dev_alloc(&w->probe_list, w->probe_cap)) != ABF_OK || (st = dev_alloc(&w->n_probe, 1)) != ABF_OK ||
         (st = dev_alloc(&w->probe_bm, uint64_t(w->probe_cap) * w->probe_stride)) != ABF_OK ||
@@ -403,6 +420,8 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
     pa.path_out = ws->path_out;
     pa.max_terms = ws->max_terms;
     pa.err = ws->err;
+    pa.dense_in_tile = 1;
+    pa.tile_cls = ws->tile_cls;
     TIMED(K_PLAN, abf::launch_plan(v, pa, s));
     abf::QueueArgs qa{ws->lcnt, ws->lpref_q, b->n_queries};
     TIMED(K_QUEUE, abf::launch_queue_scan(qa, s));
@@ -414,7 +433,7 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
         TIMED(K_PROBE_BITS, abf::launch_probe_bits(pb, ws->probe_cap, s));
     }
     abf::TileArgs ta{};
-    ta.terms = b->d_terms;
+    ta.tile_cls = ws->tile_cls;
     ta.q_off = b->d_offsets;
     ta.heavy_min = ws->heavy;
     ta.n_q = b->n_queries;
@@ -423,6 +442,7 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
     ta.out_stride = b->bitmap_stride_words;
     ta.n_words = n_words;
     ta.accumulate = 0;
+    ta.vec_ok = (reinterpret_cast<uintptr_t>(b->d_bitmaps) % 16 == 0) && (b->bitmap_stride_words % 4 == 0);
     TIMED(K_TILE, abf::launch_tile_union(v, ta, t, ix->sm_count, s));
     abf::ScatterArgs sa{};
     sa.terms = b->d_terms;
@@ -441,6 +461,7 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
         pr.qbm_words = uint32_t(ws->probe_stride);
         pr.staged_ok = 1;
         pr.d_n_probe = ws->n_probe;
+        pr.n_probe_host = ws->probe_cap;  // upper bound on the device count
         pr.out_slot = ws->probe_list;
         pr.out = b->d_bitmaps;
         pr.out_stride = b->bitmap_stride_words;
@@ -472,6 +493,7 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
 abf_status worker_plan_scratch(abf_worker* w, uint64_t n_q) {
     ABF_TRY(dev_alloc(&w->d_heavy, n_q));
     ABF_TRY(dev_alloc(&w->d_lpref, std::max<uint64_t>(w->n_keys, 1)));
+    ABF_TRY(dev_alloc(&w->d_tile_cls, std::max<uint64_t>(w->n_keys, 1)));
     ABF_TRY(dev_alloc(&w->d_lcnt, n_q));
     ABF_TRY(dev_alloc(&w->d_lpref_q, n_q + 1));
     ABF_TRY(dev_alloc(&w->d_nprobe, 1));
@@ -484,6 +506,7 @@ void worker_release(abf_worker* w) {
     dev_free(w->d_offk);
     dev_free(w->d_heavy);
     dev_free(w->d_lpref);
+    dev_free(w->d_tile_cls);
     dev_free(w->d_lcnt);
     dev_free(w->d_lpref_q);
     dev_free(w->d_nprobe);
@@ -517,6 +540,8 @@ abf_status run_sparse(const abf_worker* w, uint32_t* d_res, bool keyed, const ui
     pa.probe_cap = 0;
     pa.max_terms = w->n_keys;
     pa.err = nullptr;
+    pa.dense_in_tile = keyed ? 0 : 1;
+    pa.tile_cls = w->d_tile_cls;
     CUDA_TRY(cudaMemsetAsync(w->d_nprobe, 0, sizeof(uint32_t), s));
     TIMED(K_PLAN, abf::launch_plan(v, pa, s));
     abf::QueueArgs qa{w->d_lcnt, w->d_lpref_q, n_q};
@@ -524,7 +549,7 @@ abf_status run_sparse(const abf_worker* w, uint32_t* d_res, bool keyed, const ui
     const uint64_t n_words = n_words_of(ix->n_ads);
     if (!keyed) {
         abf::TileArgs ta{};
-        ta.terms = w->d_keys;
+        ta.tile_cls = w->d_tile_cls;
         ta.q_off = q_off;
         ta.heavy_min = w->d_heavy;
         ta.n_q = 1;
@@ -533,6 +558,7 @@ abf_status run_sparse(const abf_worker* w, uint32_t* d_res, bool keyed, const ui
         ta.out_stride = n_words;
         ta.n_words = n_words;
         ta.accumulate = 1;
+        ta.vec_ok = (reinterpret_cast<uintptr_t>(d_res) % 16 == 0) && (n_words % 4 == 0);
         TIMED(K_TILE, abf::launch_tile_union(v, ta, t, ix->sm_count, s));
     }
     abf::ScatterArgs sa{};
@@ -613,6 +639,7 @@ abf_status abf_index_build_csr(const uint64_t* offsets, const uint32_t* ads, uin
     abf::clear_error();
     if (!offsets || !out || n_terms == 0 || n_ads == 0) return fail(ABF_ERR_INVALID, "abf_index_build_csr: bad arguments");
     if (n_ads > (1u << 31)) return fail(ABF_ERR_RANGE, "n_ads above 2^31");
+    if (n_terms > (1u << 31)) return fail(ABF_ERR_RANGE, "n_terms above 2^31");
     if (offsets[0] != 0) return fail(ABF_ERR_INVALID, "offsets[0] must be 0");
     for (uint32_t t = 0; t < n_terms; ++t)
         if (offsets[t + 1] < offsets[t]) return fail(ABF_ERR_INVALID, "offsets not monotone");
@@ -675,6 +702,9 @@ abf_status abf_index_get_stats(const abf_index* ix, abf_index_stats* o) {
     o->device_bytes = ix->dev.bytes;
     o->max_list_len = ix->max_list_len;
     o->on_device = ix->on_device ? 1u : 0u;
+    o->n_dense_lists = ix->derived.n_dense;
+    o->n_directory_lists = ix->derived.n_dir;
+    o->dense_bytes = uint64_t(ix->derived.n_dense) * ix->derived.dense_stride * 4u;
     return ABF_OK;
 }
 
@@ -759,8 +789,8 @@ abf_status abf_get_tuning(const abf_index* ix, abf_tuning* out) {
 
 abf_status abf_set_tuning(abf_index* ix, const abf_tuning* t) {
     if (!ix || !t) return fail(ABF_ERR_INVALID, "null argument");
-    if (t->tile_words != 256 && t->tile_words != 512 && t->tile_words != 1024)
-        return fail(ABF_ERR_INVALID, "tile_words must be 256, 512 or 1024");
+    if (t->tile_words < 256 || t->tile_words > 16384 || (t->tile_words & (t->tile_words - 1)))
+        return fail(ABF_ERR_INVALID, "tile_words must be a power of two from 256 to 16384");
     if (t->warps_per_tile != 1 && t->warps_per_tile != 2 && t->warps_per_tile != 4 && t->warps_per_tile != 8)
         return fail(ABF_ERR_INVALID, "warps_per_tile must be 1, 2, 4 or 8");
     if (t->probe_chunk_blocks == 0 || t->probe_chunk_blocks % 128 != 0)
@@ -1054,6 +1084,15 @@ abf_status abf_query(abf_index* ix, const uint32_t* terms, uint32_t n_terms, abf
 abf_status abf_index_list_bytes(const abf_index* ix, uint64_t* h_out, uint32_t n) {
     if (!ix || !h_out || n < ix->n_terms) return fail(ABF_ERR_INVALID, "abf_index_list_bytes: bad arguments");
     std::memcpy(h_out, ix->h_term_bytes.data(), size_t(ix->n_terms) * 8);
+    return ABF_OK;
+}
+
+abf_status abf_index_list_flags(const abf_index* ix, uint32_t* h_out, uint32_t n) {
+    if (!ix || !h_out || n < ix->n_terms) return fail(ABF_ERR_INVALID, "abf_index_list_flags: bad arguments");
+    const auto& d = ix->derived;
+    for (uint32_t t = 0; t < ix->n_terms; ++t)
+        h_out[t] = (d.term_dense[t] != abf::kNone ? ABF_LIST_DENSE : 0u) |
+                   (d.term_dir[t] != abf::kNone ? ABF_LIST_DIRECTORY : 0u);
     return ABF_OK;
 }
 

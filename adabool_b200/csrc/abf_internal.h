@@ -68,6 +68,29 @@ struct HostIndex {
     uint64_t n_blocks() const { return blk_first.size(); }
 };
 
+// Tables derived from the lists at load time (not stored in the file):
+//   - dense bitmaps: a list with len * dense_div >= n_ads also gets a
+//     plain bitmap over all ads (dense_stride words, a multiple of 4); the
+//     merge kernel ORs its tile slice instead of decoding the blocks;
+//   - block directory: for long lists without a dense bitmap, dir[j] is
+//     the first block whose last id is >= j * 2^kDirShift, so a tile finds
+//     its blocks with three loads instead of two binary searches.
+constexpr uint32_t kNone = 0xffffffffu;
+constexpr uint32_t kDirShift = 13;      // directory granularity: 8192 ids = 256 words
+constexpr uint32_t kDefaultDenseDiv = 32;
+constexpr uint32_t kDirDiv = 512;       // lists with len * kDirDiv >= n_ads get a directory
+
+struct DerivedHost {
+    std::vector<uint32_t> term_dense;   // n_terms: dense bitmap index or kNone
+    std::vector<uint32_t> dense;        // n_dense * dense_stride words
+    uint64_t dense_stride = 0;
+    uint32_t n_dense = 0;
+    std::vector<uint32_t> term_dir;     // n_terms: offset into dir or kNone
+    std::vector<uint32_t> dir;          // n_dir * dir_n absolute block indices
+    uint32_t dir_n = 0;                 // entries per list: ceil(n_ads / 2^kDirShift) + 1
+    uint32_t n_dir = 0;
+};
+
 // Device copies of the same arrays.
 struct DeviceIndex {
     uint32_t* term_blk = nullptr;
@@ -77,6 +100,10 @@ struct DeviceIndex {
     uint32_t* blk_term = nullptr;
     abf_u2* blk_desc = nullptr;
     abf_u4* payload = nullptr;
+    uint32_t* term_dense = nullptr;
+    uint32_t* dense = nullptr;
+    uint32_t* term_dir = nullptr;
+    uint32_t* dir = nullptr;
     uint64_t bytes = 0;
 };
 
@@ -89,6 +116,12 @@ struct IndexView {
     const uint32_t* blk_term;
     const uint32_t* term_blk;
     const uint32_t* term_len;
+    const uint32_t* term_dense;
+    const uint32_t* dense;
+    const uint32_t* term_dir;
+    const uint32_t* dir;
+    uint64_t dense_stride;
+    uint32_t dir_n;
     uint32_t n_terms;
     uint32_t n_ads;
     uint64_t n_blocks;
@@ -100,6 +133,8 @@ struct abf_workspace;
 
 struct abf_index {
     abf::HostIndex host;          // emptied after upload unless kept
+    abf::DerivedHost derived;     // dense bitmaps + directory (host copy until uploaded)
+    uint32_t dense_div = abf::kDefaultDenseDiv;
     bool host_valid = false;      // host arrays hold the full index
     bool on_device = false;
     int device = -1;
@@ -140,5 +175,7 @@ abf_status coo_to_csr(const uint32_t* terms, const uint32_t* ads, uint64_t nnz,
                       std::vector<uint64_t>* offsets, std::vector<uint32_t>* csr_ads);
 void decode_block_host(const HostIndex& h, uint64_t b, uint32_t* out);
 int resolve_threads(int n);
+// dense bitmaps and block directory of a host index (abf_build.cpp)
+void derive_tables(const HostIndex& h, uint32_t dense_div, int n_threads, DerivedHost* out);
 
 }  // namespace abf

@@ -38,16 +38,32 @@ __device__ __forceinline__ uint32_t warp_id() { return threadIdx.x >> 5; }
 // warp's 512-byte shared buffer with one 16-byte load per lane; each lane
 // extracts its four gaps with a funnel shift, sums them, and a shuffle scan
 // over the lanes turns the gaps into ids.
-__device__ __forceinline__ void decode_block(const IndexView& ix, uint32_t b, uint4* stage, uint32_t (&id)[4],
-                                             uint32_t& cnt) {
-    const uint32_t lane = lane_id();
+// A block's descriptor and this lane's 16 bytes of its payload, loaded
+// ahead of the decode so the loads of the next block overlap the work on
+// the current one.
+struct Fetched {
+    uint4 pay;
+    uint32_t first, meta;
+};
+
+__device__ __forceinline__ Fetched fetch_block(const IndexView& ix, uint32_t b) {
+    Fetched r;
     const uint2 d = __ldg(ix.blk_desc + b);
-    const uint32_t first = __ldg(ix.blk_first + b);
-    const uint32_t bits = d.y & 63u;
-    cnt = (d.y >> 8) + 1u;
+    r.first = __ldg(ix.blk_first + b);
+    r.meta = d.y;
+    const uint32_t bits = d.y & 63u, cnt = (d.y >> 8) + 1u;
     const uint32_t units = ((cnt - 1u) * bits + 127u) >> 7;
+    r.pay = lane_id() < units ? __ldg(ix.payload + d.x + lane_id()) : make_uint4(0u, 0u, 0u, 0u);
+    return r;
+}
+
+__device__ __forceinline__ void decode_fetched(const Fetched& fb, uint4* stage, uint32_t (&id)[4], uint32_t& cnt) {
+    const uint32_t lane = lane_id();
+    const uint32_t first = fb.first;
+    const uint32_t bits = fb.meta & 63u;
+    cnt = (fb.meta >> 8) + 1u;
     __syncwarp();
-    if (lane < units) stage[lane] = __ldg(ix.payload + d.x + lane);
+    stage[lane] = fb.pay;
     __syncwarp();
     const uint32_t* w = reinterpret_cast<const uint32_t*>(stage);
     const uint32_t mask = bits >= 32u ? kFull : ((1u << bits) - 1u);
@@ -78,6 +94,11 @@ __device__ __forceinline__ void decode_block(const IndexView& ix, uint32_t b, ui
     const uint32_t base = first + (incl - run);
 #pragma unroll
     for (int k = 0; k < 4; ++k) id[k] = base + p[k];
+}
+
+__device__ __forceinline__ void decode_block(const IndexView& ix, uint32_t b, uint4* stage, uint32_t (&id)[4],
+                                             uint32_t& cnt) {
+    decode_fetched(fetch_block(ix, b), stage, id, cnt);
 }
 
 // OR the decoded ids that fall in [lo, lo + span) into a shared-memory tile.
@@ -247,17 +268,27 @@ __global__ void __launch_bounds__(256) plan_kernel(IndexView ix, PlanArgs a) {
         }
         __syncthreads();
         path = s_path;
-        const uint32_t hm = path == ABF_PATH_TILE ? 0u : (path == ABF_PATH_HYBRID ? a.hybrid_min : kNoHeavy);
         const bool probe = path == ABF_PATH_PROBE;
+        // merge threshold: TILE merges every list, HYBRID the long ones,
+        // UNION only those with a dense bitmap, PROBE none
+        const uint32_t hm = path == ABF_PATH_TILE ? 0u
+                            : path == ABF_PATH_HYBRID ? a.hybrid_min
+                            : probe ? kNoHeavy : kDenseOnly;
         uint32_t carry = 0;
         for (uint64_t c0 = qb; c0 < qe; c0 += 256) {
             const uint64_t i = c0 + tid;
-            uint32_t cnt = 0;
+            uint32_t cnt = 0, cls = kNone;
             if (i < qe && !probe) {
                 const uint32_t t = a.terms[i];
-                if (t < ix.n_terms && __ldg(ix.term_len + t) < hm)
-                    cnt = __ldg(ix.term_blk + t + 1) - __ldg(ix.term_blk + t);
+                if (t < ix.n_terms) {
+                    const uint32_t d = a.dense_in_tile ? __ldg(ix.term_dense + t) : kNone;
+                    const uint32_t len = __ldg(ix.term_len + t);
+                    if (d != kNone) cls = kDenseFlag | d;
+                    else if (len >= hm) cls = t;
+                    else cnt = __ldg(ix.term_blk + t + 1) - __ldg(ix.term_blk + t);
+                }
             }
+            if (i < qe && a.tile_cls) a.tile_cls[i] = cls;
             uint32_t tot;
             const uint32_t ex = block_excl_scan<256>(cnt, s_warp, &tot);
             if (i < qe) a.term_lpref[i] = carry + ex;
@@ -322,65 +353,153 @@ __global__ void __launch_bounds__(256) probe_bits_kernel(ProbeBitsArgs a) {
 // ---------------------------------------------------------------------------
 // list-union, merge variant
 // ---------------------------------------------------------------------------
+// Blocks [lo, lo + cnt) of a list that overlap the ids [lo_id, hi_id):
+// three loads from the list's directory when it has one, else two binary
+// searches over the block bounds. dj0/dj1 are the directory rows of lo_id
+// and of the unclipped tile end.
+__device__ __forceinline__ void tile_block_range(const IndexView& ix, uint32_t term, uint32_t lo_id, uint32_t hi_id,
+                                                 uint32_t dj0, uint32_t dj1, uint32_t& lo, uint32_t& cnt) {
+    const uint32_t b0 = __ldg(ix.term_blk + term), b1 = __ldg(ix.term_blk + term + 1);
+    const uint32_t dofs = __ldg(ix.term_dir + term);
+    uint32_t hi;
+    if (dofs != kNone) {
+        lo = __ldg(ix.dir + dofs + dj0);
+        hi = __ldg(ix.dir + dofs + dj1);  // first block ending at or after the tile end
+        if (hi < b1 && __ldg(ix.blk_first + hi) < hi_id) ++hi;  // it straddles the tile end
+    } else {
+        lo = lower_bound_g(ix.blk_last, b0, b1, lo_id);
+        hi = lower_bound_g(ix.blk_first, lo, b1, hi_id);
+    }
+    cnt = hi > lo ? hi - lo : 0u;
+}
+
+// slot s of the chunk's prefix array with s_pref[s] <= f < s_pref[s+1]
+template <int NT>
+__device__ __forceinline__ uint32_t find_slot(const uint32_t* s_pref, uint32_t f) {
+    uint32_t a0 = 0, a1 = NT;
+    while (a1 - a0 > 1) {
+        const uint32_t m = (a0 + a1) >> 1;
+        if (s_pref[m] <= f) a0 = m; else a1 = m;
+    }
+    return a0;
+}
+
 template <int W, int NW>
 __global__ void __launch_bounds__(NW * 32) tile_union_kernel(IndexView ix, TileArgs a) {
     constexpr int NT = NW * 32;
     constexpr uint32_t SPAN = uint32_t(W) * 32u;
-    __shared__ uint32_t tile[W];
+    extern __shared__ __align__(16) uint32_t tile[];  // W words, dynamic (up to 64 KB)
     __shared__ __align__(16) uint4 stage[NW][32];
     __shared__ uint32_t s_lo[NT];
     __shared__ uint32_t s_pref[NT + 1];
+    __shared__ uint32_t s_dense[NT];
     __shared__ uint32_t s_warp[32];
+    __shared__ uint32_t s_ndense;
     const uint32_t tid = threadIdx.x, warp = warp_id();
     const uint64_t items = uint64_t(a.n_q) * a.n_tiles;
+    uint4* tile4 = reinterpret_cast<uint4*>(tile);
     for (uint64_t item = blockIdx.x; item < items; item += gridDim.x) {
-        const uint32_t q = uint32_t(item / a.n_tiles);
-        const uint32_t t = uint32_t(item - uint64_t(q) * a.n_tiles);
+        // tile-major order: the CTAs resident together work on one region of
+        // the ad space for many queries, so the blocks and dense slices of
+        // lists those queries share are read from L2
+        const uint32_t t = uint32_t(item / a.n_q);
+        const uint32_t q = uint32_t(item - uint64_t(t) * a.n_q);
         const uint32_t lo_id = t * SPAN;
         const uint32_t hi_id = (uint64_t(lo_id) + SPAN > ix.n_ads) ? ix.n_ads : lo_id + SPAN;
+        const uint32_t dj0 = lo_id >> kDirShift;
+        uint32_t dj1 = uint32_t((uint64_t(lo_id) + SPAN) >> kDirShift);
+        if (dj1 > ix.dir_n - 1) dj1 = ix.dir_n - 1;
         const uint32_t hm = a.heavy_min ? a.heavy_min[q] : a.heavy_all;
         const uint64_t qb = a.q_off[q], qe = a.q_off[q + 1];
-        if (a.accumulate && (hm == kNoHeavy || qb == qe)) continue;  // nothing to OR in
         uint32_t* dst = a.out + uint64_t(q) * a.out_stride + uint64_t(t) * W;
         const uint64_t left = a.n_words - uint64_t(t) * W;
         const uint32_t nw = left < uint64_t(W) ? uint32_t(left) : uint32_t(W);
+        if (hm == kNoHeavy || qb == qe) {  // nothing to merge: leave or zero the tile
+            if (!a.accumulate)
+                for (uint32_t i = tid; i < nw; i += NT) dst[i] = 0u;
+            continue;
+        }
         for (uint32_t i = tid; i < uint32_t(W); i += NT) tile[i] = (a.accumulate && i < nw) ? dst[i] : 0u;
+        if (tid == 0) s_ndense = 0;
         __syncthreads();
-        if (hm != kNoHeavy) {
-            for (uint64_t c0 = qb; c0 < qe; c0 += NT) {
-                const uint64_t i = c0 + tid;
-                uint32_t lo = 0, cnt = 0;
-                if (i < qe) {
-                    const uint32_t term = a.terms[i];
-                    if (term < ix.n_terms && __ldg(ix.term_len + term) >= hm) {
-                        const uint32_t b0 = __ldg(ix.term_blk + term), b1 = __ldg(ix.term_blk + term + 1);
-                        lo = lower_bound_g(ix.blk_last, b0, b1, lo_id);
-                        const uint32_t hi = lower_bound_g(ix.blk_first, lo, b1, hi_id);
-                        cnt = hi - lo;
+        for (uint64_t c0 = qb; c0 < qe; c0 += NT) {
+            const uint64_t i = c0 + tid;
+            uint32_t lo = 0, cnt = 0;
+            const uint32_t cls = i < qe ? __ldg(a.tile_cls + i) : kNone;
+            if (cls != kNone) {
+                if (cls & kDenseFlag) s_dense[atomicAdd(&s_ndense, 1u)] = cls & ~kDenseFlag;
+                else tile_block_range(ix, cls, lo_id, hi_id, dj0, dj1, lo, cnt);
+            }
+            uint32_t total;
+            const uint32_t ex = block_excl_scan<NT>(cnt, s_warp, &total);
+            s_lo[tid] = lo;
+            s_pref[tid] = ex;
+            if (tid == NT - 1) s_pref[NT] = ex + cnt;
+            __syncthreads();
+            // dense lists: OR their slice of this tile, 16 bytes per thread and
+            // slot, four lists' loads in flight at once; finished before any
+            // decode warp starts its shared atomics
+            const uint32_t nd = s_ndense;
+            if (nd) {
+                const uint4* base = reinterpret_cast<const uint4*>(ix.dense + uint64_t(t) * W);
+                const uint64_t st4 = ix.dense_stride / 4;
+                for (uint32_t j = tid; j * 4u < nw; j += NT) {
+                    uint4 acc = tile4[j];
+                    uint32_t k = 0;
+                    for (; k + 4 <= nd; k += 4) {
+                        const uint4 v0 = __ldg(base + s_dense[k] * st4 + j);
+                        const uint4 v1 = __ldg(base + s_dense[k + 1] * st4 + j);
+                        const uint4 v2 = __ldg(base + s_dense[k + 2] * st4 + j);
+                        const uint4 v3 = __ldg(base + s_dense[k + 3] * st4 + j);
+                        acc.x |= v0.x | v1.x | v2.x | v3.x;
+                        acc.y |= v0.y | v1.y | v2.y | v3.y;
+                        acc.z |= v0.z | v1.z | v2.z | v3.z;
+                        acc.w |= v0.w | v1.w | v2.w | v3.w;
                     }
+                    for (; k < nd; ++k) {
+                        const uint4 v = __ldg(base + s_dense[k] * st4 + j);
+                        acc.x |= v.x; acc.y |= v.y; acc.z |= v.z; acc.w |= v.w;
+                    }
+                    tile4[j] = acc;
                 }
-                uint32_t total;
-                const uint32_t ex = block_excl_scan<NT>(cnt, s_warp, &total);
-                s_lo[tid] = lo;
-                s_pref[tid] = ex;
-                if (tid == NT - 1) s_pref[NT] = ex + cnt;
-                __syncthreads();
-                for (uint32_t f = warp; f < total; f += NW) {
-                    // slot s: s_pref[s] <= f < s_pref[s+1]
-                    uint32_t a0 = 0, a1 = NT;
-                    while (a1 - a0 > 1) {
-                        const uint32_t m = (a0 + a1) >> 1;
-                        if (s_pref[m] <= f) a0 = m; else a1 = m;
+            }
+            __syncthreads();
+            // decode the blocks: warp w takes a contiguous share of the flat
+            // block range, finds its first (slot, block) once and walks on,
+            // keeping the next block's loads in flight
+            const uint32_t per = (total + NW - 1) / NW;
+            uint32_t f = warp * per;
+            const uint32_t fend = f + per < total ? f + per : total;
+            if (f < fend) {
+                uint32_t s = find_slot<NT>(s_pref, f);
+                uint32_t j = f - s_pref[s];
+                Fetched nxt = fetch_block(ix, s_lo[s] + j);
+                while (f < fend) {
+                    const Fetched cur = nxt;
+                    if (++f < fend) {
+                        if (++j == s_pref[s + 1] - s_pref[s]) {  // next list with blocks in this tile
+                            j = 0;
+                            do {
+                                ++s;
+                            } while (s_pref[s + 1] == s_pref[s]);
+                        }
+                        nxt = fetch_block(ix, s_lo[s] + j);
                     }
-                    const uint32_t b = s_lo[a0] + (f - s_pref[a0]);
                     uint32_t id[4], cnt_b;
-                    decode_block(ix, b, stage[warp], id, cnt_b);
+                    decode_fetched(cur, stage[warp], id, cnt_b);
                     or_tile(tile, lo_id, SPAN, id, cnt_b);
                 }
-                __syncthreads();
             }
+            if (tid == 0) s_ndense = 0;
+            __syncthreads();
         }
-        for (uint32_t i = tid; i < nw; i += NT) dst[i] = tile[i];
+        if (a.vec_ok) {
+            uint4* d4 = reinterpret_cast<uint4*>(dst);
+            for (uint32_t j = tid; j * 4u + 3u < nw; j += NT) d4[j] = tile4[j];
+            for (uint32_t i = (nw & ~3u) + tid; i < nw; i += NT) dst[i] = tile[i];
+        } else {
+            for (uint32_t i = tid; i < nw; i += NT) dst[i] = tile[i];
+        }
         __syncthreads();
     }
 }
@@ -453,7 +572,9 @@ __global__ void __launch_bounds__(NW * 32) probe_kernel(IndexView ix, ProbeArgs 
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t s_fail;
     const uint32_t tid = threadIdx.x, lane = lane_id(), warp = warp_id();
-    const uint32_t n_probe = a.d_n_probe ? *a.d_n_probe : a.n_probe_host;
+    // the device counter also counts queries demoted past the slot capacity
+    uint32_t n_probe = a.n_probe_host;
+    if (a.d_n_probe && *a.d_n_probe < n_probe) n_probe = *a.d_n_probe;
     if (n_probe == 0 || ix.n_blocks == 0) return;
     if (tid == 0) {
         mbar_init(&bar, 1);
@@ -638,43 +759,88 @@ __global__ void __launch_bounds__(kScanNT) scan_kernel(const uint32_t* in, uint6
     if (tile == last_tile && tid == 0) out[n] = s_prefix + agg;
 }
 
+// One CTA per (bitmap, 2048-word chunk): the chunk is staged in shared
+// memory, its 64 units of 32 words are counted and scanned once, then every
+// warp expands its units on its own, one word at a time with one lane per
+// bit: the lanes holding set bits store their ids to consecutive output
+// addresses (rank = popcount of the lower bits), so each store instruction
+// writes one contiguous run and no lane loops over bits.
+constexpr uint32_t kUnits = kCompactChunkWords / 32;
+static_assert(kUnits == 64, "the unit scan below covers 64 units with one warp");
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
 __global__ void __launch_bounds__(256) write_ids_kernel(CompactArgs a) {
-    __shared__ uint32_t s_ids[256 * 32];
-    __shared__ uint32_t s_warp[32];
-    const uint32_t tid = threadIdx.x;
+    __shared__ __align__(16) uint32_t s_words[kCompactChunkWords];
+    __shared__ uint32_t s_unit[kUnits];
+    const uint32_t tid = threadIdx.x, lane = lane_id(), warp = warp_id();
+    const uint32_t lt = lanemask_lt();
     const uint64_t n_words = (a.n_bits + 31) / 32;
     const uint64_t items = uint64_t(a.n_q) * a.n_chunks;
     for (uint64_t item = blockIdx.x; item < items; item += gridDim.x) {
         const uint32_t q = uint32_t(item / a.n_chunks);
         const uint32_t c = uint32_t(item - uint64_t(q) * a.n_chunks);
         const uint32_t* bm = a.bm + uint64_t(q) * a.stride;
-        uint64_t out = a.offsets[item];
+        const uint64_t out = a.offsets[item];
         if (c == 0 && tid == 0) {
             if (a.id_offsets) a.id_offsets[q] = out;
             if (a.id_counts) a.id_counts[q] = a.offsets[item + a.n_chunks] - out;
             if (a.id_offsets && q == a.n_q - 1) a.id_offsets[a.n_q] = a.offsets[items];
         }
         const uint64_t w0 = uint64_t(c) * kCompactChunkWords;
-        const uint64_t w1 = w0 + kCompactChunkWords < n_words ? w0 + kCompactChunkWords : n_words;
-        for (uint64_t r0 = w0; r0 < w1; r0 += 256) {
-            const uint64_t w = r0 + tid;
-            uint32_t v = w < w1 ? masked_word(bm, w, a.n_bits) : 0u;
-            uint32_t tot;
-            uint32_t pos = block_excl_scan<256>(__popc(v), s_warp, &tot);
-            const uint32_t idbase = uint32_t(w * 32u);
-            while (v) {
-                const uint32_t b = __ffs(v) - 1u;
-                v &= v - 1u;
-                s_ids[pos++] = idbase + b;
-            }
-            __syncthreads();
-            for (uint32_t k = tid; k < tot; k += 256) {
-                const uint64_t o = out + k;
-                if (o < a.capacity) a.ids[o] = s_ids[k];
-            }
-            out += tot;
-            __syncthreads();
+        const uint32_t nwc = uint32_t(w0 + kCompactChunkWords < n_words ? kCompactChunkWords : n_words - w0);
+        for (uint32_t i = tid; i < kCompactChunkWords; i += 256)
+            s_words[i] = i < nwc ? masked_word(bm, w0 + i, a.n_bits) : 0u;
+        __syncthreads();
+        for (uint32_t u = warp; u < kUnits; u += 8) {
+            uint32_t s = __popc(s_words[u * 32u + lane]);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(kFull, s, o);
+            if (lane == 0) s_unit[u] = s;
         }
+        __syncthreads();
+        if (warp == 0) {
+            const uint32_t v0 = s_unit[2 * lane], v1 = s_unit[2 * lane + 1];
+            uint32_t x = v0 + v1;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(kFull, x, o);
+                if (lane >= uint32_t(o)) x += y;
+            }
+            const uint32_t ex = x - v0 - v1;
+            s_unit[2 * lane] = ex;
+            s_unit[2 * lane + 1] = ex + v0;
+        }
+        __syncthreads();
+        for (uint32_t u = warp; u < kUnits; u += 8) {
+            const uint32_t v = s_words[u * 32u + lane];
+            const uint32_t cnt = __popc(v);
+            uint32_t x = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(kFull, x, o);
+                if (lane >= uint32_t(o)) x += y;
+            }
+            const uint32_t ex = x - cnt;
+            const uint64_t o0 = out + s_unit[u];
+            const uint32_t idb = uint32_t((w0 + u * 32u) * 32u);
+            uint32_t nz = __ballot_sync(kFull, v != 0u);
+            while (nz) {
+                const uint32_t w = __ffs(nz) - 1u;
+                nz &= nz - 1u;
+                const uint32_t word = __shfl_sync(kFull, v, w);
+                const uint32_t pos = __shfl_sync(kFull, ex, w);
+                if ((word >> lane) & 1u) {
+                    const uint64_t o = o0 + pos + __popc(word & lt);
+                    if (o < a.capacity) a.ids[o] = idb + w * 32u + lane;
+                }
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -695,6 +861,12 @@ IndexView view_of(const abf_index* ix) {
     v.blk_term = ix->dev.blk_term;
     v.term_blk = ix->dev.term_blk;
     v.term_len = ix->dev.term_len;
+    v.term_dense = ix->dev.term_dense;
+    v.dense = ix->dev.dense;
+    v.term_dir = ix->dev.term_dir;
+    v.dir = ix->dev.dir;
+    v.dense_stride = ix->derived.dense_stride;
+    v.dir_n = ix->derived.dir_n;
     v.n_terms = ix->n_terms;
     v.n_ads = ix->n_ads;
     v.n_blocks = ix->n_blocks;
@@ -728,15 +900,26 @@ cudaError_t launch_probe_bits(const ProbeBitsArgs& a, uint32_t probe_cap, cudaSt
     return cudaGetLastError();
 }
 
+template <int W, int NW>
+static cudaError_t tile_launch(const IndexView& v, const TileArgs& a, int grid, cudaStream_t s) {
+    constexpr int smem = W * 4;
+    if (smem > 48 * 1024) {
+        // opt in to more than 48 KB of dynamic shared memory (per device)
+        cudaError_t e = cudaFuncSetAttribute(tile_union_kernel<W, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+    }
+    tile_union_kernel<W, NW><<<grid, NW * 32, smem, s>>>(v, a);
+    return cudaGetLastError();
+}
+
 template <int W>
 static cudaError_t tile_dispatch_w(const IndexView& v, const TileArgs& a, uint32_t nw, int grid, cudaStream_t s) {
     switch (nw) {
-        case 1: tile_union_kernel<W, 1><<<grid, 32, 0, s>>>(v, a); break;
-        case 2: tile_union_kernel<W, 2><<<grid, 64, 0, s>>>(v, a); break;
-        case 4: tile_union_kernel<W, 4><<<grid, 128, 0, s>>>(v, a); break;
-        default: tile_union_kernel<W, 8><<<grid, 256, 0, s>>>(v, a); break;
+        case 1: return tile_launch<W, 1>(v, a, grid, s);
+        case 2: return tile_launch<W, 2>(v, a, grid, s);
+        case 4: return tile_launch<W, 4>(v, a, grid, s);
+        default: return tile_launch<W, 8>(v, a, grid, s);
     }
-    return cudaGetLastError();
 }
 
 cudaError_t launch_tile_union(const IndexView& v, const TileArgs& a, const abf_tuning& t, int sm_count,
@@ -751,6 +934,10 @@ cudaError_t launch_tile_union(const IndexView& v, const TileArgs& a, const abf_t
     switch (t.tile_words) {
         case 256: e = tile_dispatch_w<256>(v, a, nw, grid, s); break;
         case 512: e = tile_dispatch_w<512>(v, a, nw, grid, s); break;
+        case 2048: e = tile_dispatch_w<2048>(v, a, nw, grid, s); break;
+        case 4096: e = tile_dispatch_w<4096>(v, a, nw, grid, s); break;
+        case 8192: e = tile_dispatch_w<8192>(v, a, nw, grid, s); break;
+        case 16384: e = tile_dispatch_w<16384>(v, a, nw, grid, s); break;
         default: e = tile_dispatch_w<1024>(v, a, nw, grid, s); break;
     }
     count_launch();

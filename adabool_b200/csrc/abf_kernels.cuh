@@ -27,6 +27,7 @@
 namespace abf {
 
 constexpr uint32_t kNoHeavy = 0xffffffffu;   // heavy_min meaning "merge no list"
+constexpr uint32_t kDenseOnly = 0xfffffffeu; // heavy_min meaning "merge only the dense-bitmap lists"
 constexpr uint32_t kCompactChunkWords = 2048; // bitmap words per compaction work item
 constexpr uint32_t kProbeGroup = 32;          // probe queries tested per pass
 constexpr uint32_t kScanTile = 2048;          // elements per decoupled look-back tile
@@ -53,7 +54,12 @@ struct PlanArgs {
     uint8_t* path_out;        // out (optional): resolved path per query
     uint64_t max_terms;       // term slots of the scratch arrays; queries past it get no work
     uint32_t* err;            // device error flag (optional)
+    int dense_in_tile;        // 1: dense-bitmap lists go to the merge kernel, 0: scattered too
+    uint32_t* tile_cls;       // out: per term slot, what the merge kernel does with it
+                              // (kNone: nothing, kDenseFlag | d: dense bitmap d, else the term)
 };
+
+constexpr uint32_t kDenseFlag = 0x80000000u;
 
 struct QueueArgs {
     const uint64_t* q_light_cnt;
@@ -72,7 +78,7 @@ struct ProbeBitsArgs {
 };
 
 struct TileArgs {
-    const uint32_t* terms;
+    const uint32_t* tile_cls;  // per term slot, from the plan kernel
     const uint64_t* q_off;
     const uint32_t* heavy_min; // per query (null: heavy_all for every query)
     uint32_t heavy_all;
@@ -82,6 +88,7 @@ struct TileArgs {
     uint64_t out_stride;      // words between query bitmaps
     uint64_t n_words;         // words of one bitmap
     int accumulate;           // 1: OR into the existing bitmap, 0: overwrite
+    int vec_ok;               // out 16-byte aligned and out_stride % 4 == 0
 };
 
 struct ScatterArgs {
@@ -101,8 +108,8 @@ struct ProbeArgs {
     uint64_t qbm_stride;
     uint32_t qbm_words;        // readable words per bitmap
     int staged_ok;             // qbm 16-byte aligned and stride % 4 == 0
-    const uint32_t* d_n_probe; // device count (null: n_probe_host)
-    uint32_t n_probe_host;
+    const uint32_t* d_n_probe; // device count, clamped to n_probe_host (null: n_probe_host)
+    uint32_t n_probe_host;     // probe bitmaps available
     const uint32_t* out_slot;  // probe slot -> output bitmap index (null: identity)
     uint32_t* out;
     uint64_t out_stride;

@@ -101,30 +101,31 @@ class Index:
 
     # ---- construction -------------------------------------------------
     @staticmethod
-    def _opts(device, host_only, keep_host, n_threads):
+    def _opts(device, host_only, keep_host, n_threads, dense_div=0):
+        """dense_div: 0 = library default, None = no dense bitmaps."""
         flags = (N.BUILD_HOST_ONLY if host_only else 0) | (N.BUILD_KEEP_HOST if keep_host else 0)
-        return N.BuildOpts(device, flags, n_threads)
+        return N.BuildOpts(device, flags, n_threads, N.DENSE_NONE if dense_div is None else int(dense_div))
 
     @classmethod
     def from_coo(cls, terms, ads, n_terms: int, n_ads: int, device: int = 0, host_only: bool = False,
-                 keep_host: bool = False, n_threads: int = 0) -> "Index":
+                 keep_host: bool = False, n_threads: int = 0, dense_div=0) -> "Index":
         t, a = _u32(terms), _u32(ads)
         if t.shape != a.shape:
             raise ValueError("terms and ads differ in length")
         h = C.c_void_p()
-        o = cls._opts(device, host_only, keep_host, n_threads)
+        o = cls._opts(device, host_only, keep_host, n_threads, dense_div)
         check(lib().abf_index_build_coo(ptr(t, N.u32p), ptr(a, N.u32p), t.size, n_terms, n_ads, C.byref(o),
                                         C.byref(h)))
         return cls(h)
 
     @classmethod
     def from_csr(cls, offsets, ads, n_terms: int, n_ads: int, device: int = 0, host_only: bool = False,
-                 keep_host: bool = False, n_threads: int = 0) -> "Index":
+                 keep_host: bool = False, n_threads: int = 0, dense_div=0) -> "Index":
         off, a = _u64(offsets), _u32(ads)
         if off.size != n_terms + 1:
             raise ValueError("offsets must have n_terms + 1 entries")
         h = C.c_void_p()
-        o = cls._opts(device, host_only, keep_host, n_threads)
+        o = cls._opts(device, host_only, keep_host, n_threads, dense_div)
         check(lib().abf_index_build_csr(ptr(off, N.u64p), ptr(a, N.u32p), n_terms, n_ads, C.byref(o),
                                         C.byref(h)))
         return cls(h)
@@ -141,9 +142,10 @@ class Index:
         return cls.from_coo(arr[:, 0], arr[:, 1], n_terms, n_ads, **kw)
 
     @classmethod
-    def load(cls, path: str, device: int = 0, host_only: bool = False, keep_host: bool = False) -> "Index":
+    def load(cls, path: str, device: int = 0, host_only: bool = False, keep_host: bool = False,
+             dense_div=0) -> "Index":
         h = C.c_void_p()
-        o = cls._opts(device, host_only, keep_host, 0)
+        o = cls._opts(device, host_only, keep_host, 0, dense_div)
         check(lib().abf_index_load(str(path).encode(), C.byref(o), C.byref(h)))
         return cls(h)
 
@@ -190,6 +192,12 @@ class Index:
         """Compressed bytes of each term's list (payload + 16 B metadata per block)."""
         out = np.empty(self.n_terms, dtype=np.uint64)
         check(lib().abf_index_list_bytes(self._h, ptr(out, N.u64p), self.n_terms))
+        return out
+
+    def list_flags(self) -> np.ndarray:
+        """Per-term flags: 1 = also a dense bitmap, 2 = per-tile block directory."""
+        out = np.empty(self.n_terms, dtype=np.uint32)
+        check(lib().abf_index_list_flags(self._h, ptr(out, N.u32p), self.n_terms))
         return out
 
     def profile(self, on: bool = True):

@@ -236,19 +236,30 @@ def run_ours(args, rank, world, dev):
         e2e = run_e2e(args, ix, sbs, ws, bms, ids, idoff, stride, path, dev, world, n_q)
 
     # ---- algorithmic bytes (roofline numerator) ----
-    lbytes = ix.list_bytes().astype(np.float64)
-    hm = ix.tuning.heavy_min_len
-    heavy_t = lens >= (hm if path in (ab.PATH_HYBRID, ab.PATH_AUTO) else (0 if path == ab.PATH_TILE else 1 << 62))
-    qb = lbytes[qterms]
-    q_heavy = np.add.reduceat(np.where(heavy_t[qterms], qb, 0.0), qoff[:-1].astype(np.int64)) if qterms.size else 0
-    q_all = np.add.reduceat(qb, qoff[:-1].astype(np.int64)) if qterms.size else 0
-    empty = np.diff(qoff) == 0
-    q_heavy = np.where(empty, 0.0, q_heavy)
-    q_all = np.where(empty, 0.0, q_all)
+    # a list is read in the representation its kernel uses: the merge kernel
+    # reads a dense bitmap (n_ads/8 bytes) where the list has one, blocks
+    # (payload + 16 B metadata each) otherwise; the scatter kernel reads blocks
     bm_bytes = L.n_ads / 8.0
+    lbytes = ix.list_bytes().astype(np.float64)
+    dense_t = (ix.list_flags() & 1) != 0
+    hm = ix.tuning.heavy_min_len
+    merged_t = {ab.PATH_HYBRID: dense_t | (lens >= hm), ab.PATH_TILE: np.ones_like(dense_t),
+                ab.PATH_UNION: dense_t, ab.PATH_AUTO: dense_t,
+                ab.PATH_PROBE: np.zeros_like(dense_t)}[path]
+    read_t = np.where(dense_t & merged_t, bm_bytes, lbytes)
+    seg = qoff[:-1].astype(np.int64)
+    empty = np.diff(qoff) == 0
+
+    def per_query(x):
+        if not qterms.size:
+            return np.zeros(n_q)
+        return np.where(empty, 0.0, np.add.reduceat(x, seg))
+
+    q_merge = per_query(np.where(merged_t[qterms], read_t[qterms], 0.0))
+    q_all = per_query(read_t[qterms])
     alg = {
-        "tile_union": float(np.sum(q_heavy)) + n_q * bm_bytes,
-        "scatter_union": float(np.sum(q_all - q_heavy)),
+        "tile_union": float(np.sum(q_merge)) + n_q * bm_bytes,
+        "scatter_union": float(np.sum(q_all - q_merge)),
         "compact_count": n_q * bm_bytes,
         "compact_write": n_q * bm_bytes + 4.0 * float(counts.sum()),
     }

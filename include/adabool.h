@@ -75,6 +75,8 @@ typedef struct abf_build_opts {
     int device;          /* CUDA device ordinal (ignored with ABF_BUILD_HOST_ONLY) */
     uint32_t flags;      /* ABF_BUILD_* */
     int n_threads;       /* host threads for the build; <= 0 = all cores */
+    uint32_t dense_div;  /* a list with len * dense_div >= n_ads also gets a dense
+                            bitmap, merged without decoding; 0 = 32, 0xffffffff = none */
 } abf_build_opts;
 
 typedef struct abf_index_stats {
@@ -86,6 +88,9 @@ typedef struct abf_index_stats {
     uint64_t device_bytes;      /* all device arrays of the index */
     uint32_t max_list_len;
     uint32_t on_device;         /* 1 if the device copy exists */
+    uint32_t n_dense_lists;     /* lists that also have a dense bitmap */
+    uint32_t n_directory_lists; /* lists with a per-tile block directory */
+    uint64_t dense_bytes;       /* bytes of the dense bitmaps */
 } abf_index_stats;
 
 /* Build from COO pairs (terms[i], ads[i]), i < nnz. Pairs may be in any
@@ -134,7 +139,7 @@ abf_status abf_index_to_device(abf_index* index, int device);
 /* ------------------------------------------------------------------ */
 
 typedef struct abf_tuning {
-    uint32_t tile_words;      /* words per merge tile: 256, 512 or 1024 */
+    uint32_t tile_words;      /* words per merge tile: a power of two, 256 .. 16384 */
     uint32_t warps_per_tile;  /* warps that share one tile's lists: 1, 2, 4 or 8 */
     uint32_t heavy_min_len;   /* HYBRID: lists with >= this many postings are merged
                                  per tile, shorter lists are scattered */
@@ -262,6 +267,14 @@ abf_status abf_query(abf_index* index, const uint32_t* terms, uint32_t n_terms, 
 /* Compressed bytes of every term's list (n_terms entries): payload plus
  * 16 bytes of block metadata per block. No reference counterpart. */
 abf_status abf_index_list_bytes(const abf_index* index, uint64_t* h_out, uint32_t n);
+
+/* Per-term representation flags (n_terms entries): ABF_LIST_DENSE when the
+ * list also has a dense bitmap of (n_ads + 31) / 32 words that the merge
+ * kernel reads instead of its blocks, ABF_LIST_DIRECTORY when it has a
+ * per-tile block directory. No reference counterpart. */
+#define ABF_LIST_DENSE 1u
+#define ABF_LIST_DIRECTORY 2u
+abf_status abf_index_list_flags(const abf_index* index, uint32_t* h_out, uint32_t n);
 
 /* Kernel timing. While enabled, every kernel this index launches is
  * bracketed by CUDA events on the stream it is launched on;

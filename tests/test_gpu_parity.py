@@ -43,7 +43,11 @@ def small(dev):
            np.array([heavy], np.uint32),                         # one long list
            np.arange(0, spec.n_terms, 3, dtype=np.uint32)]       # a third of all terms
     ix = Index.from_csr(off, ads, spec.n_terms, spec.n_ads, device=0, keep_host=True)
-    return dict(spec=spec, off=off, ads=ads, qs=qs, ix=ix, n_words=(spec.n_ads + 31) // 32)
+    # same lists without dense bitmaps: every long list merged from its blocks
+    # through the directory
+    ix_nodense = Index.from_csr(off, ads, spec.n_terms, spec.n_ads, device=0, dense_div=None)
+    assert ix.stats()["n_dense_lists"] > 0 and ix_nodense.stats()["n_directory_lists"] > 0
+    return dict(spec=spec, off=off, ads=ads, qs=qs, ix=ix, ix_nodense=ix_nodense, n_words=(spec.n_ads + 31) // 32)
 
 
 def test_decode_roundtrip_host(small):
@@ -52,10 +56,11 @@ def test_decode_roundtrip_host(small):
         assert np.array_equal(ix.decode_list(t), ads[off[t]:off[t + 1]])
 
 
+@pytest.mark.parametrize("variant", ["ix", "ix_nodense"])
 @pytest.mark.parametrize("path", PATHS)
-def test_query_every_path(small, path):
+def test_query_every_path(small, path, variant):
     torch = _torch()
-    ix, n_words = small["ix"], small["n_words"]
+    ix, n_words = small[variant], small["n_words"]
     n_ads = small["spec"].n_ads
     bm = torch.full((n_words,), -1, dtype=torch.int32, device="cuda")  # garbage: must be overwritten
     ids = torch.empty(n_ads + 1, dtype=torch.int32, device="cuda")
@@ -107,7 +112,7 @@ def test_batch_mixed_paths_and_probe_overflow(small):
         ix.set_tuning(probe_cap=old)
 
 
-@pytest.mark.parametrize("tile_words", [256, 512, 1024])
+@pytest.mark.parametrize("tile_words", [256, 512, 1024, 4096, 16384])
 @pytest.mark.parametrize("warps", [1, 2, 4, 8])
 def test_tuning_sweep_identical(small, tile_words, warps):
     torch = _torch()
