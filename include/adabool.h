@@ -218,6 +218,23 @@ abf_status abf_collect_ids(abf_index* index, const uint32_t* d_bitmap, uint64_t 
                            uint32_t* d_ids, uint64_t ids_capacity, uint64_t* d_count,
                            void* stream);
 
+/* Allocation-free variant of abf_collect_ids, with no counterpart in the
+ * reference. For callers that may not allocate device memory when they
+ * need the ids: an engine that owns all device memory and forbids plugins
+ * to allocate, a serving thread that cannot afford cudaMalloc's possible
+ * device-wide synchronisation, code that must not hit out-of-memory in
+ * the middle of a request. Needs no index and calls no cudaMalloc/cudaFree:
+ * its scratch is one static device array (about 200 KB per device, kept
+ * until the process exits) sized for at most ABF_NOALLOC_MAX_BITS bits;
+ * larger bitmaps are refused with ABF_ERR_CAPACITY. The first call on a
+ * device looks up that array's device address (cudaGetSymbolAddress) and
+ * should come before any stream capture. Every call on a device shares the
+ * array: calls whose work can overlap on the GPU race and must be ordered
+ * by the caller (one stream, or events). Results equal abf_collect_ids. */
+#define ABF_NOALLOC_MAX_BITS (1ull << 30)
+abf_status abf_collect_ids_noalloc(const uint32_t* d_bitmap, uint64_t n_bits, uint32_t* d_ids,
+                                   uint64_t ids_capacity, uint64_t* d_count, void* stream);
+
 /* ------------------------------------------------------------------ */
 /* Native batched API (no reference counterpart beyond the batch paths) */
 /* ------------------------------------------------------------------ */
