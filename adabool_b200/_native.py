@@ -90,6 +90,7 @@ PROTOTYPES = {
     "abf_index_to_device": [vp, C.c_int],
     "abf_get_tuning": [vp, C.POINTER(Tuning)],
     "abf_set_tuning": [vp, C.POINTER(Tuning)],
+    "abf_index_set_dense_div": [vp, C.c_uint32],
     "abf_prepare_sparse": [vp, u32p, C.c_uint64, C.POINTER(vp)],
     "abf_prepare_dense": [vp, C.c_uint64, u8p, C.POINTER(vp)],
     "abf_prepare_batch": [vp, C.c_uint64, C.c_uint64, u8p, C.POINTER(vp)],

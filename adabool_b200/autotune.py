@@ -28,6 +28,7 @@ KNOBS = {
     "warps_per_tile": [1, 2, 4, 8],
     "ctas_per_sm": [2, 4, 6, 8],
     "scatter_blocks_per_warp": [1, 2, 4, 8],
+    "dense_div": [16, 32, 64, 128, 256],  # lists with len * dense_div >= n_ads get dense bitmaps
 }
 
 
@@ -49,6 +50,8 @@ class TuneResult:
 
 def apply(index, path_or_dict):
     d = path_or_dict if isinstance(path_or_dict, dict) else json.loads(Path(path_or_dict).read_text())["best"]
+    if "dense_div" in d and d["dense_div"] != getattr(index, "dense_div", None):
+        index.set_dense_div(d["dense_div"])
     index.set_tuning(**{k: v for k, v in d.items() if k in dict(N.Tuning._fields_)})
 
 
@@ -98,6 +101,12 @@ def autotune(index, q_off: np.ndarray, q_terms: np.ndarray, path: int = N.PATH_H
     space = dict(KNOBS if knobs is None else knobs)
     space.setdefault("heavy_min_len", heavy_candidates(index.n_ads))
     cur = index.tuning.as_dict()
+    cur["dense_div"] = int(getattr(index, "dense_div", 32))
+    tuning_knobs = [k for k in space if k != "dense_div"]
+
+    def apply_cur():
+        index.set_tuning(**{k: cur[k] for k in tuning_knobs})
+
     trials = []
     best_ms = run.time_ms(reps)
     trials.append({"tuning": dict(cur), "ms": best_ms})
@@ -110,7 +119,10 @@ def autotune(index, q_off: np.ndarray, q_terms: np.ndarray, path: int = N.PATH_H
                 cand = dict(cur)
                 cand[knob] = v
                 try:
-                    index.set_tuning(**{knob: v})
+                    if knob == "dense_div":  # representation: rebuilds the dense bitmaps
+                        index.set_dense_div(v)
+                    else:
+                        index.set_tuning(**{knob: v})
                 except N.AbfError:
                     continue
                 ms = run.time_ms(reps)
@@ -119,8 +131,12 @@ def autotune(index, q_off: np.ndarray, q_terms: np.ndarray, path: int = N.PATH_H
                     print(f"  {knob}={v}: {ms:.3f} ms (best {best_ms:.3f})", flush=True)
                 if ms < best_ms * 0.995:
                     best_ms, cur, improved = ms, cand, True
-                index.set_tuning(**{k: cur[k] for k in space})
+                if knob == "dense_div" and cur["dense_div"] != v:
+                    index.set_dense_div(cur["dense_div"])
+                apply_cur()
         if not improved:
             break
-    index.set_tuning(**{k: cur[k] for k in space})
-    return TuneResult(best={k: cur[k] for k in cur}, best_ms=best_ms, trials=trials)
+    apply_cur()
+    if "dense_div" in space:
+        index.dense_div = cur["dense_div"]
+    return TuneResult(best=dict(cur), best_ms=best_ms, trials=trials)

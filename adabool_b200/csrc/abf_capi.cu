@@ -733,24 +733,79 @@ abf_status abf_index_decode_list(const abf_index* ix, uint32_t term, uint32_t* h
     API_END
 }
 
+}  // extern "C"
+
+namespace {
+// host copy of the list arrays from the device (for an index built without
+// ABF_BUILD_KEEP_HOST)
+abf_status fetch_host(const abf_index* ix, abf::HostIndex* h) {
+    h->n_terms = ix->n_terms;
+    h->n_ads = ix->n_ads;
+    h->n_postings = ix->n_postings;
+    h->max_list_len = ix->max_list_len;
+    CUDA_TRY(cudaSetDevice(ix->device));
+    ABF_TRY(download_vec(h->term_blk, ix->dev.term_blk, uint64_t(ix->n_terms) + 1));
+    ABF_TRY(download_vec(h->term_len, ix->dev.term_len, ix->n_terms));
+    ABF_TRY(download_vec(h->blk_first, ix->dev.blk_first, ix->n_blocks));
+    ABF_TRY(download_vec(h->blk_last, ix->dev.blk_last, ix->n_blocks));
+    ABF_TRY(download_vec(h->blk_term, ix->dev.blk_term, ix->n_blocks));
+    ABF_TRY(download_vec(h->blk_desc, ix->dev.blk_desc, ix->n_blocks));
+    ABF_TRY(download_vec(h->payload, ix->dev.payload, ix->payload_units));
+    return ABF_OK;
+}
+}  // namespace
+
+extern "C" {
+
 abf_status abf_index_save(const abf_index* ix, const char* path) {
     API_BEGIN
     if (!ix || !path) return fail(ABF_ERR_INVALID, "null argument");
     if (ix->host_valid) return abf::save_host(ix->host, path);
     abf::HostIndex h;
-    h.n_terms = ix->n_terms;
-    h.n_ads = ix->n_ads;
-    h.n_postings = ix->n_postings;
-    h.max_list_len = ix->max_list_len;
-    CUDA_TRY(cudaSetDevice(ix->device));
-    ABF_TRY(download_vec(h.term_blk, ix->dev.term_blk, uint64_t(ix->n_terms) + 1));
-    ABF_TRY(download_vec(h.term_len, ix->dev.term_len, ix->n_terms));
-    ABF_TRY(download_vec(h.blk_first, ix->dev.blk_first, ix->n_blocks));
-    ABF_TRY(download_vec(h.blk_last, ix->dev.blk_last, ix->n_blocks));
-    ABF_TRY(download_vec(h.blk_term, ix->dev.blk_term, ix->n_blocks));
-    ABF_TRY(download_vec(h.blk_desc, ix->dev.blk_desc, ix->n_blocks));
-    ABF_TRY(download_vec(h.payload, ix->dev.payload, ix->payload_units));
+    ABF_TRY(fetch_host(ix, &h));
     return abf::save_host(h, path);
+    API_END
+}
+
+abf_status abf_index_set_dense_div(abf_index* ix, uint32_t dense_div) {
+    API_BEGIN
+    if (!ix) return fail(ABF_ERR_INVALID, "null index");
+    abf::HostIndex tmp;
+    const abf::HostIndex* h = &ix->host;
+    if (!ix->host_valid) {
+        ABF_TRY(fetch_host(ix, &tmp));
+        h = &tmp;
+    }
+    abf::DerivedHost d;
+    abf::derive_tables(*h, dense_div, 0, &d);
+    if (ix->on_device) {
+        CUDA_TRY(cudaSetDevice(ix->device));
+        CUDA_TRY(cudaDeviceSynchronize());
+        auto& dv = ix->dev;
+        const uint64_t old = 4ull * (ix->derived.term_dense.size() + ix->derived.term_dir.size()) +
+                             4ull * uint64_t(ix->derived.n_dense) * ix->derived.dense_stride +
+                             4ull * uint64_t(ix->derived.n_dir) * ix->derived.dir_n;
+        dev_free(dv.term_dense);
+        dev_free(dv.dense);
+        dev_free(dv.term_dir);
+        dev_free(dv.dir);
+        dv.bytes = dv.bytes > old ? dv.bytes - old : 0;
+        abf_status st;
+        if ((st = upload_vec(&dv.term_dense, d.term_dense, &dv.bytes)) != ABF_OK ||
+            (st = upload_vec(&dv.dense, d.dense, &dv.bytes)) != ABF_OK ||
+            (st = upload_vec(&dv.term_dir, d.term_dir, &dv.bytes)) != ABF_OK ||
+            (st = upload_vec(&dv.dir, d.dir, &dv.bytes)) != ABF_OK) {
+            free_device(ix);
+            return st;
+        }
+        if (!ix->host_valid) {
+            d.dense = std::vector<uint32_t>();
+            d.dir = std::vector<uint32_t>();
+        }
+    }
+    ix->derived = std::move(d);
+    ix->dense_div = dense_div;
+    return ABF_OK;
     API_END
 }
 

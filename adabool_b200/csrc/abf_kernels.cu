@@ -535,16 +535,13 @@ __global__ void __launch_bounds__(NW * 32) scatter_kernel(IndexView ix, ScatterA
         uint64_t i = i0;
         uint32_t j = r - a.term_lpref[i];
         uint32_t* out = a.out + uint64_t(a.out_slot ? a.out_slot[q] : q) * a.out_stride;
-        for (uint64_t f = f0; f < f1;) {
-            const uint32_t nb = (i + 1 < qe ? a.term_lpref[i + 1] : qtot) - a.term_lpref[i];
-            if (j < nb) {
-                const uint32_t b = __ldg(ix.term_blk + a.terms[i]) + j;
-                uint32_t id[4], cnt;
-                decode_block(ix, b, stage[warp], id, cnt);
-                or_global(out, ix.n_ads, id, cnt);
-                ++j;
-                ++f;
-            } else {
+        // (i, j) is a scattered block of query q; the walk moves to the next
+        // one, crossing into later terms and queries as they run out
+        auto advance = [&]() {
+            ++j;
+            for (;;) {
+                const uint32_t nb = (i + 1 < qe ? a.term_lpref[i + 1] : qtot) - a.term_lpref[i];
+                if (j < nb) return;
                 ++i;
                 j = 0;
                 if (i >= qe) {
@@ -558,6 +555,20 @@ __global__ void __launch_bounds__(NW * 32) scatter_kernel(IndexView ix, ScatterA
                     out = a.out + uint64_t(a.out_slot ? a.out_slot[q] : q) * a.out_stride;
                 }
             }
+        };
+        Fetched nxt = fetch_block(ix, __ldg(ix.term_blk + a.terms[i]) + j);
+        uint32_t* nxt_out = out;
+        for (uint64_t f = f0; f < f1; ++f) {
+            const Fetched cur = nxt;
+            uint32_t* cur_out = nxt_out;
+            if (f + 1 < f1) {  // next block's loads in flight during this decode
+                advance();
+                nxt = fetch_block(ix, __ldg(ix.term_blk + a.terms[i]) + j);
+                nxt_out = out;
+            }
+            uint32_t id[4], cnt;
+            decode_fetched(cur, stage[warp], id, cnt);
+            or_global(cur_out, ix.n_ads, id, cnt);
         }
     }
 }
@@ -774,11 +785,26 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     return m;
 }
 
+// bulk copy shared -> global (TMA engine), completion tracked per thread
+__device__ __forceinline__ void bulk_s2g(void* gdst, const void* ssrc, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst), "r"(smem_addr(ssrc)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+constexpr uint32_t kIdBuf = 1024 + 8;  // one unit's ids plus the 16-byte alignment head
+
 __global__ void __launch_bounds__(256) write_ids_kernel(CompactArgs a) {
     __shared__ __align__(16) uint32_t s_words[kCompactChunkWords];
     __shared__ uint32_t s_unit[kUnits];
+    __shared__ __align__(16) uint32_t s_buf[8][kIdBuf];
     const uint32_t tid = threadIdx.x, lane = lane_id(), warp = warp_id();
     const uint32_t lt = lanemask_lt();
+    const bool ids16 = (reinterpret_cast<uintptr_t>(a.ids) & 15u) == 0;
+    uint32_t* buf = s_buf[warp];
     const uint64_t n_words = (a.n_bits + 31) / 32;
     const uint64_t items = uint64_t(a.n_q) * a.n_chunks;
     for (uint64_t item = blockIdx.x; item < items; item += gridDim.x) {
@@ -827,21 +853,59 @@ __global__ void __launch_bounds__(256) write_ids_kernel(CompactArgs a) {
             }
             const uint32_t ex = x - cnt;
             const uint64_t o0 = out + s_unit[u];
-            const uint32_t idb = uint32_t((w0 + u * 32u) * 32u);
+            const uint32_t my_id = uint32_t((w0 + u * 32u) * 32u) + lane;
             uint32_t nz = __ballot_sync(kFull, v != 0u);
-            while (nz) {
-                const uint32_t w = __ffs(nz) - 1u;
-                nz &= nz - 1u;
-                const uint32_t word = __shfl_sync(kFull, v, w);
-                const uint32_t pos = __shfl_sync(kFull, ex, w);
-                if ((word >> lane) & 1u) {
-                    const uint64_t o = o0 + pos + __popc(word & lt);
-                    if (o < a.capacity) a.ids[o] = idb + w * 32u + lane;
+            uint32_t* dst = a.ids + o0;
+            const uint32_t tot = __shfl_sync(kFull, x, 31);
+            if (ids16 && tot >= 64 && o0 + tot <= a.capacity) {
+                // dense unit: ids go to the warp's shared buffer at their
+                // 16-byte-aligned output position, the aligned middle leaves
+                // by one bulk copy, the ragged ends by plain stores
+                const uint32_t head = uint32_t(o0 & 3u);
+                if (lane == 0) bulk_wait_read_all();  // the previous unit's copy has read the buffer
+                __syncwarp();
+                while (nz) {
+                    const uint32_t w = __ffs(nz) - 1u;
+                    nz &= nz - 1u;
+                    const uint32_t word = __shfl_sync(kFull, v, w);
+                    const uint32_t pos = __shfl_sync(kFull, ex, w);
+                    if ((word >> lane) & 1u) buf[head + pos + __popc(word & lt)] = my_id + w * 32u;
+                }
+                fence_proxy_async();  // these shared writes before the async-proxy read
+                __syncwarp();
+                const uint32_t end = head + tot;
+                const uint32_t mid_hi = end & ~3u;
+                uint32_t* gbase = dst - head;  // 16-byte aligned
+                if (lane == 0 && mid_hi > 4u) {
+                    bulk_s2g(gbase + 4, buf + 4, (mid_hi - 4u) * 4u);
+                    bulk_commit();
+                }
+                if (lane >= head && lane < 4u) gbase[lane] = buf[lane];
+                if (mid_hi + lane < end) gbase[mid_hi + lane] = buf[mid_hi + lane];
+            } else if (o0 + tot <= a.capacity) {  // whole unit fits: no per-id check
+                while (nz) {
+                    const uint32_t w = __ffs(nz) - 1u;
+                    nz &= nz - 1u;
+                    const uint32_t word = __shfl_sync(kFull, v, w);
+                    const uint32_t pos = __shfl_sync(kFull, ex, w);
+                    if ((word >> lane) & 1u) dst[pos + __popc(word & lt)] = my_id + w * 32u;
+                }
+            } else {
+                while (nz) {
+                    const uint32_t w = __ffs(nz) - 1u;
+                    nz &= nz - 1u;
+                    const uint32_t word = __shfl_sync(kFull, v, w);
+                    const uint32_t pos = __shfl_sync(kFull, ex, w);
+                    if ((word >> lane) & 1u) {
+                        const uint64_t o = o0 + pos + __popc(word & lt);
+                        if (o < a.capacity) a.ids[o] = my_id + w * 32u;
+                    }
                 }
             }
         }
         __syncthreads();
     }
+    if (lane == 0) bulk_wait_all();
 }
 
 inline int grid_for(uint64_t items, int sm_count, uint32_t per_sm) {

@@ -98,6 +98,7 @@ class Index:
         self.n_terms = st.n_terms
         self.n_ads = st.n_ads
         self.n_words = (self.n_ads + 31) // 32
+        self.dense_div = 32  # library default; set_dense_div / the builder's dense_div change it
 
     # ---- construction -------------------------------------------------
     @staticmethod
@@ -219,6 +220,11 @@ class Index:
     @tuning.setter
     def tuning(self, t: N.Tuning):
         check(lib().abf_set_tuning(self._h, C.byref(t)))
+
+    def set_dense_div(self, dense_div):
+        """Rebuild the dense bitmaps for lists with len * dense_div >= n_ads (None: no bitmaps)."""
+        check(lib().abf_index_set_dense_div(self._h, N.DENSE_NONE if dense_div is None else int(dense_div)))
+        self.dense_div = dense_div
 
     def set_tuning(self, **kw):
         t = self.tuning

@@ -55,6 +55,7 @@ def parse():
     p.add_argument("--queries", type=int, default=0, help="override the query count")
     p.add_argument("--sub-batch", type=int, default=64)
     p.add_argument("--path", default="hybrid", choices=["auto", "probe", "union", "hybrid", "tile", "planner"])
+    p.add_argument("--no-autotune", action="store_true", help="keep the library's default tuning")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -170,6 +171,15 @@ def run_ours(args, rank, world, dev):
     stride = (n_words + 3) // 4 * 4
     path = {"auto": ab.PATH_AUTO, "probe": ab.PATH_PROBE, "union": ab.PATH_UNION, "hybrid": ab.PATH_HYBRID,
             "tile": ab.PATH_TILE, "planner": ab.PATH_AUTO}[args.path]
+    tune_info = None
+    if not args.no_autotune:
+        # untimed setup: the project's autotuner picks tile width, warps per
+        # tile, the merge/scatter switch, dense-bitmap threshold, CTAs per SM
+        from adabool_b200 import autotune as AT
+        t0 = time.time()
+        tr = AT.autotune(ix, qoff, qterms, path=path, sub_batch=args.sub_batch, sample=512, device=dev)
+        tune_info = {"seconds": round(time.time() - t0, 1), "trials": len(tr.trials),
+                     "sample_ms": round(tr.best_ms, 3), "dense_div": tr.best.get("dense_div")}
     sbs = split(qoff, qterms, args.sub_batch)
     max_terms = max(int(s[3].size) for s in sbs) + 1
     # id capacity: the bound min(n_ads, sum of list lengths) per query
@@ -289,7 +299,8 @@ def run_ours(args, rank, world, dev):
         "config": {"workload": f"{cfg.name}: {L.n_terms} terms x {L.n_ads} ads, {st['n_postings']} postings; "
                                f"{n_q} queries/rank, sub-batches of {args.sub_batch}",
                    "path": args.path, "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (no flush)",
-                   "index_bytes": st["device_bytes"], "tuning": ix.tuning.as_dict()},
+                   "index_bytes": ix.stats()["device_bytes"],
+                   "tuning": dict(ix.tuning.as_dict(), dense_div=ix.dense_div), "autotune": tune_info},
         "postings_per_s": round(postings * world / (ms_step / 1e3), 1),
         "postings_raw_gbs": round(4 * postings * world / (ms_step / 1e3) / 1e9, 1),
         "algorithmic_gbs": round(total_alg * world / (ms_step / 1e3) / 1e9, 1),

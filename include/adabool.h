@@ -155,6 +155,11 @@ typedef struct abf_tuning {
 abf_status abf_get_tuning(const abf_index* index, abf_tuning* out);
 abf_status abf_set_tuning(abf_index* index, const abf_tuning* t);
 
+/* Rebuilds the dense bitmaps (and block directory) for a new dense_div
+ * (see abf_build_opts; 0xffffffff = none) and re-uploads them; synchronises
+ * the device. The merge threshold heavy_min_len is left as it is. */
+abf_status abf_index_set_dense_div(abf_index* index, uint32_t dense_div);
+
 /* ------------------------------------------------------------------ */
 /* Reference-shaped operator API (prepare a worker, run it into d_res)  */
 /* ------------------------------------------------------------------ */

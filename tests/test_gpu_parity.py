@@ -133,6 +133,28 @@ def test_tuning_sweep_identical(small, tile_words, warps):
         ix.set_tuning(**saved)
 
 
+@pytest.mark.parametrize("variant", ["ix", "ix_nodense"])
+def test_dense_div_rebuild(small, variant):
+    """Changing the dense-bitmap threshold at run time (host copy kept, or
+    fetched back from the device) keeps every result bit-exact."""
+    torch = _torch()
+    ix, n_words = small[variant], small["n_words"]
+    bm = torch.empty(n_words, dtype=torch.int32, device="cuda")
+    try:
+        for dd in (8, 256, None, 32):
+            ix.set_dense_div(dd)
+            st = ix.stats()
+            assert (st["n_dense_lists"] == 0) == (dd is None)
+            for q in small["qs"][::4]:
+                for path in (ab.PATH_HYBRID, ab.PATH_UNION):
+                    ix.query(q, bm, path=path)
+                    torch.cuda.synchronize()
+                    assert np.array_equal(bm.cpu().numpy().view(np.uint32),
+                                          expected(small["off"], small["ads"], q, n_words)[1])
+    finally:
+        ix.set_dense_div(32 if variant == "ix" else None)
+
+
 def test_reference_api_or_semantics(small):
     """Prepare + ListUnion_* OR into the caller's buffer like the reference."""
     torch = _torch()
