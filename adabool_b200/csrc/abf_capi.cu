@@ -204,13 +204,14 @@ uint64_t round4(uint64_t x) { return (x + 3) & ~uint64_t(3); }
 
 void default_tuning(abf_index* ix) {
     abf_tuning& t = ix->tuning;
-    t.tile_words = 1024;
+    t.tile_words = 2048;
     t.warps_per_tile = 8;
-    // HYBRID merges per tile the lists holding at least 1/32 of the ads (the
-    // ones that also get dense bitmaps); measured on the 2^24-ad workload,
-    // decoding shorter lists inside the tiles loses to scattering them, as a
-    // tile holds only a block or two of each
-    t.heavy_min_len = uint32_t(std::max<uint64_t>((uint64_t(ix->n_ads) + 31) / 32, abf::kBlock));
+    // HYBRID merges per tile the lists that have dense bitmaps (at the
+    // default dense_div, those holding at least 1/128 of the ads); measured on
+    // the 2^24-ad workload, decoding shorter lists inside the tiles loses to
+    // scattering them, as a tile holds only a block or two of each
+    const uint32_t div = ix->dense_div && ix->dense_div != abf::kNone ? ix->dense_div : abf::kDefaultDenseDiv;
+    t.heavy_min_len = uint32_t(std::max<uint64_t>((uint64_t(ix->n_ads) + div - 1) / div, abf::kBlock));
     t.probe_chunk_blocks = 256;
     t.scatter_blocks_per_warp = 8;
     t.ctas_per_sm = 6;

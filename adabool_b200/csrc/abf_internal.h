@@ -77,7 +77,7 @@ struct HostIndex {
 //     its blocks with three loads instead of two binary searches.
 constexpr uint32_t kNone = 0xffffffffu;
 constexpr uint32_t kDirShift = 13;      // directory granularity: 8192 ids = 256 words
-constexpr uint32_t kDefaultDenseDiv = 32;
+constexpr uint32_t kDefaultDenseDiv = 128;
 constexpr uint32_t kDirDiv = 512;       // lists with len * kDirDiv >= n_ads get a directory
 
 struct DerivedHost {

@@ -441,26 +441,44 @@ __global__ void __launch_bounds__(NW * 32) tile_union_kernel(IndexView ix, TileA
             // decode warp starts its shared atomics
             const uint32_t nd = s_ndense;
             if (nd) {
+                // each thread keeps VG of its 16-byte slots in registers and
+                // issues VG x KT independent loads per step (KT lists at once)
+                constexpr int V = (W / 4 + NT - 1) / NT;
+                constexpr int VG = V < 4 ? V : 4;
+                constexpr int KT = VG >= 4 ? 2 : (VG == 2 ? 4 : 8);
                 const uint4* base = reinterpret_cast<const uint4*>(ix.dense + uint64_t(t) * W);
                 const uint64_t st4 = ix.dense_stride / 4;
-                for (uint32_t j = tid; j * 4u < nw; j += NT) {
-                    uint4 acc = tile4[j];
-                    uint32_t k = 0;
-                    for (; k + 4 <= nd; k += 4) {
-                        const uint4 v0 = __ldg(base + s_dense[k] * st4 + j);
-                        const uint4 v1 = __ldg(base + s_dense[k + 1] * st4 + j);
-                        const uint4 v2 = __ldg(base + s_dense[k + 2] * st4 + j);
-                        const uint4 v3 = __ldg(base + s_dense[k + 3] * st4 + j);
-                        acc.x |= v0.x | v1.x | v2.x | v3.x;
-                        acc.y |= v0.y | v1.y | v2.y | v3.y;
-                        acc.z |= v0.z | v1.z | v2.z | v3.z;
-                        acc.w |= v0.w | v1.w | v2.w | v3.w;
+                for (int vg = 0; vg < V; vg += VG) {
+                    uint4 acc[VG];
+#pragma unroll
+                    for (int v = 0; v < VG; ++v) {
+                        const uint32_t j = tid + uint32_t(vg + v) * NT;
+                        acc[v] = j * 4u < nw ? tile4[j] : make_uint4(0u, 0u, 0u, 0u);
                     }
-                    for (; k < nd; ++k) {
-                        const uint4 v = __ldg(base + s_dense[k] * st4 + j);
-                        acc.x |= v.x; acc.y |= v.y; acc.z |= v.z; acc.w |= v.w;
+                    for (uint32_t k = 0; k < nd; k += KT) {
+                        const uint4* src[KT];
+#pragma unroll
+                        for (int e = 0; e < KT; ++e)
+                            src[e] = base + uint64_t(s_dense[k + e < nd ? k + e : k]) * st4;
+#pragma unroll
+                        for (int v = 0; v < VG; ++v) {
+                            const uint32_t j = tid + uint32_t(vg + v) * NT;
+                            if (j * 4u < nw) {
+                                uint4 x[KT];
+#pragma unroll
+                                for (int e = 0; e < KT; ++e) x[e] = __ldg(src[e] + j);
+#pragma unroll
+                                for (int e = 0; e < KT; ++e) {
+                                    acc[v].x |= x[e].x; acc[v].y |= x[e].y; acc[v].z |= x[e].z; acc[v].w |= x[e].w;
+                                }
+                            }
+                        }
                     }
-                    tile4[j] = acc;
+#pragma unroll
+                    for (int v = 0; v < VG; ++v) {
+                        const uint32_t j = tid + uint32_t(vg + v) * NT;
+                        if (j * 4u < nw) tile4[j] = acc[v];
+                    }
                 }
             }
             __syncthreads();

@@ -98,7 +98,7 @@ class Index:
         self.n_terms = st.n_terms
         self.n_ads = st.n_ads
         self.n_words = (self.n_ads + 31) // 32
-        self.dense_div = 32  # library default; set_dense_div / the builder's dense_div change it
+        self.dense_div = 128  # library default; set_dense_div / the builder's dense_div change it
 
     # ---- construction -------------------------------------------------
     @staticmethod

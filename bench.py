@@ -56,6 +56,7 @@ def parse():
     p.add_argument("--sub-batch", type=int, default=64)
     p.add_argument("--path", default="hybrid", choices=["auto", "probe", "union", "hybrid", "tile", "planner"])
     p.add_argument("--no-autotune", action="store_true", help="keep the library's default tuning")
+    p.add_argument("--tuning", default="", help="apply a saved autotuner result (JSON) instead of tuning")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -172,7 +173,11 @@ def run_ours(args, rank, world, dev):
     path = {"auto": ab.PATH_AUTO, "probe": ab.PATH_PROBE, "union": ab.PATH_UNION, "hybrid": ab.PATH_HYBRID,
             "tile": ab.PATH_TILE, "planner": ab.PATH_AUTO}[args.path]
     tune_info = None
-    if not args.no_autotune:
+    if args.tuning:
+        from adabool_b200 import autotune as AT
+        AT.apply(ix, args.tuning)
+        tune_info = {"from": args.tuning}
+    elif not args.no_autotune:
         # untimed setup: the project's autotuner picks tile width, warps per
         # tile, the merge/scatter switch, dense-bitmap threshold, CTAs per SM
         from adabool_b200 import autotune as AT

@@ -76,7 +76,7 @@ typedef struct abf_build_opts {
     uint32_t flags;      /* ABF_BUILD_* */
     int n_threads;       /* host threads for the build; <= 0 = all cores */
     uint32_t dense_div;  /* a list with len * dense_div >= n_ads also gets a dense
-                            bitmap, merged without decoding; 0 = 32, 0xffffffff = none */
+                            bitmap, merged without decoding; 0 = 128, 0xffffffff = none */
 } abf_build_opts;
 
 typedef struct abf_index_stats {

@@ -152,7 +152,7 @@ def test_dense_div_rebuild(small, variant):
                     assert np.array_equal(bm.cpu().numpy().view(np.uint32),
                                           expected(small["off"], small["ads"], q, n_words)[1])
     finally:
-        ix.set_dense_div(32 if variant == "ix" else None)
+        ix.set_dense_div(128 if variant == "ix" else None)
 
 
 def test_reference_api_or_semantics(small):

@@ -83,10 +83,10 @@ def test_dense_and_directory_tables():
     lens = np.diff(off)
     ix = Index.from_csr(off, ads, spec.n_terms, spec.n_ads, host_only=True)
     st = ix.stats()
-    n_dense = int((lens * 32 >= spec.n_ads).sum())
+    n_dense = int((lens * 128 >= spec.n_ads).sum())
     assert st["n_dense_lists"] == n_dense > 0
     assert st["dense_bytes"] == n_dense * ((spec.n_ads // 32 + 3) // 4 * 4) * 4
-    assert st["n_directory_lists"] == int(((lens * 512 >= spec.n_ads) & (lens * 32 < spec.n_ads) & (lens > 128)).sum())
+    assert st["n_directory_lists"] == int(((lens * 512 >= spec.n_ads) & (lens * 128 < spec.n_ads) & (lens > 128)).sum())
     none = Index.from_csr(off, ads, spec.n_terms, spec.n_ads, host_only=True, dense_div=None)
     assert none.stats()["n_dense_lists"] == 0 and none.stats()["n_directory_lists"] > st["n_directory_lists"]
 
@@ -134,7 +134,7 @@ def test_device_calls_on_host_only_index_fail_cleanly():
 def test_tuning_validation():
     ix = Index.from_csr([0, 2], [1, 5], 1, 10, host_only=True)
     t = ix.tuning
-    assert t.tile_words in (256, 512, 1024) and t.heavy_min_len >= 128
+    assert t.tile_words in (256, 512, 1024, 2048, 4096, 8192, 16384) and t.heavy_min_len >= 128
     for bad in ({"tile_words": 300}, {"warps_per_tile": 3}, {"probe_chunk_blocks": 100}, {"ctas_per_sm": 0}):
         with pytest.raises(ab.AbfError):
             ix.set_tuning(**bad)
