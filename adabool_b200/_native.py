@@ -26,6 +26,12 @@ PATH_AUTO, PATH_PROBE, PATH_UNION, PATH_HYBRID, PATH_TILE = 0, 1, 2, 3, 4
 PATH_NAMES = {PATH_AUTO: "auto", PATH_PROBE: "probe", PATH_UNION: "union", PATH_HYBRID: "hybrid",
               PATH_TILE: "tile"}
 
+PLANNER_FEATURES = 16
+PLANNER_HIDDEN = 64
+PLANNER_OUTPUTS = 3
+PLANNER_PARAMS = 2 * 16 + 64 * 16 + 64 + 64 * 64 + 64 + 3 * 64 + 3
+PLANNER_PATHS = (1, 2, 3)  # outputs 0..2 predict PROBE, UNION, HYBRID
+
 BUILD_HOST_ONLY = 1
 BUILD_KEEP_HOST = 2
 QCOUNT_UNIFORM = 0
@@ -107,6 +113,12 @@ PROTOTYPES = {
     "abf_workspace_check": [vp, vp],
     "abf_batch_run": [vp, vp, C.POINTER(Batch), vp],
     "abf_query": [vp, u32p, C.c_uint32, C.c_int, vp, vp, C.c_uint64, vp, vp],
+    "abf_planner_features": [vp, vp, vp, C.c_uint32, vp, vp],
+    "abf_planner_set": [vp, vp],
+    "abf_planner_predict": [vp, vp, vp, C.c_uint32, vp, vp, vp],
+    "abf_mlp_forward": [vp, vp, C.c_uint32, vp, vp],
+    "abf_mlp_grad": [vp, vp, vp, vp, C.c_uint32, vp, vp, vp],
+    "abf_mlp_adam": [vp, vp, vp, vp, C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float, vp],
     "abf_index_list_bytes": [vp, u64p, C.c_uint32],
     "abf_index_list_flags": [vp, u32p, C.c_uint32],
     "abf_profile_enable": [vp, C.c_int],

@@ -56,10 +56,11 @@ using abf::fail;
 namespace {
 
 // ---- kernel timing (abf_profile_enable / abf_profile_read) ----
-enum Kid { K_PLAN, K_QUEUE, K_PROBE_BITS, K_TILE, K_SCATTER, K_PROBE, K_COUNT, K_SCAN, K_WRITE, K_NKERNELS };
+enum Kid { K_PLAN, K_QUEUE, K_PROBE_BITS, K_TILE, K_SCATTER, K_PROBE, K_COUNT, K_SCAN, K_WRITE, K_PLANNER,
+           K_NKERNELS };
 const char* const kKernelNames[K_NKERNELS] = {"plan",   "queue_scan",    "probe_bits",   "tile_union",
                                               "scatter_union", "probe", "compact_count", "compact_scan",
-                                              "compact_write"};
+                                              "compact_write", "planner"};
 
 struct Profiler {
     struct Rec {
@@ -138,6 +139,7 @@ struct abf_workspace {
     uint32_t* scan_counter = nullptr;
     uint64_t* id_off = nullptr;
     uint8_t* path_out = nullptr;
+    uint8_t* auto_paths = nullptr;  // planner choices for ABF_PATH_AUTO batches
     uint32_t* err = nullptr;
     uint32_t* q_terms = nullptr;  // single-query staging (abf_query)
     uint64_t* q_off = nullptr;
@@ -232,8 +234,16 @@ void free_device(abf_index* ix) {
     dev_free(d.dense);
     dev_free(d.term_dir);
     dev_free(d.dir);
+    dev_free(d.term_cbytes);
+    dev_free(d.planner);
     d.bytes = 0;
     ix->on_device = false;
+}
+
+std::vector<uint32_t> cbytes32(const abf_index* ix) {
+    std::vector<uint32_t> v(ix->h_term_bytes.size());
+    for (size_t i = 0; i < v.size(); ++i) v[i] = uint32_t(std::min<uint64_t>(ix->h_term_bytes[i], 0xffffffffull));
+    return v;
 }
 
 abf_status upload(abf_index* ix, int device) {
@@ -256,7 +266,8 @@ abf_status upload(abf_index* ix, int device) {
         (st = upload_vec(&d.term_dense, ix->derived.term_dense, &d.bytes)) != ABF_OK ||
         (st = upload_vec(&d.dense, ix->derived.dense, &d.bytes)) != ABF_OK ||
         (st = upload_vec(&d.term_dir, ix->derived.term_dir, &d.bytes)) != ABF_OK ||
-        (st = upload_vec(&d.dir, ix->derived.dir, &d.bytes)) != ABF_OK) {
+        (st = upload_vec(&d.dir, ix->derived.dir, &d.bytes)) != ABF_OK ||
+        (st = upload_vec(&d.term_cbytes, cbytes32(ix), &d.bytes)) != ABF_OK) {
         free_device(ix);
         return st;
     }
@@ -322,6 +333,7 @@ void ws_release(abf_workspace* w) {
     dev_free(w->scan_counter);
     dev_free(w->id_off);
     dev_free(w->path_out);
+    dev_free(w->auto_paths);
     dev_free(w->err);
     dev_free(w->q_terms);
     dev_free(w->q_off);
@@ -345,6 +357,7 @@ abf_status ws_alloc(abf_index* ix, uint32_t max_q, uint64_t max_terms, uint64_t 
         (st = dev_alloc(&w->scan_status, abf::scan_tiles(chunks))) != ABF_OK ||
         (st = dev_alloc(&w->scan_counter, 1)) != ABF_OK || (st = dev_alloc(&w->id_off, uint64_t(max_q) + 1)) != ABF_OK ||
         (st = dev_alloc(&w->path_out, max_q)) != ABF_OK || (st = dev_alloc(&w->err, 1)) != ABF_OK ||
+        (st = dev_alloc(&w->auto_paths, max_q)) != ABF_OK ||
         (st = dev_alloc(&w->q_terms, max_terms)) != ABF_OK || (st = dev_alloc(&w->q_off, 2)) != ABF_OK) {
         ws_release(w);
         return st;
@@ -423,6 +436,12 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
     pa.err = ws->err;
     pa.dense_in_tile = 1;
     pa.tile_cls = ws->tile_cls;
+    if (!b->d_paths && b->path == ABF_PATH_AUTO && ix->dev.planner) {
+        // learned planner: per-query path from the fused feature + MLP kernel
+        TIMED(K_PLANNER, abf::launch_planner(v, ix->dev.planner, b->d_terms, b->d_offsets, b->n_queries,
+                                             t.heavy_min_len, ix->n_postings, nullptr, nullptr, ws->auto_paths, s));
+        pa.paths = ws->auto_paths;
+    }
     TIMED(K_PLAN, abf::launch_plan(v, pa, s));
     abf::QueueArgs qa{ws->lcnt, ws->lpref_q, b->n_queries};
     TIMED(K_QUEUE, abf::launch_queue_scan(qa, s));
@@ -1141,6 +1160,74 @@ abf_status abf_index_list_bytes(const abf_index* ix, uint64_t* h_out, uint32_t n
     if (!ix || !h_out || n < ix->n_terms) return fail(ABF_ERR_INVALID, "abf_index_list_bytes: bad arguments");
     std::memcpy(h_out, ix->h_term_bytes.data(), size_t(ix->n_terms) * 8);
     return ABF_OK;
+}
+
+abf_status abf_planner_features(abf_index* ix, const uint32_t* d_terms, const uint64_t* d_offsets, uint32_t n_q,
+                                float* d_features, void* stream) {
+    API_BEGIN
+    ABF_TRY(need_device(ix));
+    if (n_q && (!d_terms || !d_offsets || !d_features)) return fail(ABF_ERR_INVALID, "abf_planner_features: null pointer");
+    CUDA_TRY(cudaSetDevice(ix->device));
+    CUDA_TRY(abf::launch_planner(abf::view_of(ix), nullptr, d_terms, d_offsets, n_q, ix->tuning.heavy_min_len,
+                                 ix->n_postings, d_features, nullptr, nullptr, static_cast<cudaStream_t>(stream)));
+    return ABF_OK;
+    API_END
+}
+
+abf_status abf_planner_set(abf_index* ix, const float* h_params) {
+    API_BEGIN
+    ABF_TRY(need_device(ix));
+    CUDA_TRY(cudaSetDevice(ix->device));
+    if (!h_params) {
+        CUDA_TRY(cudaDeviceSynchronize());
+        dev_free(ix->dev.planner);
+        return ABF_OK;
+    }
+    if (!ix->dev.planner) ABF_TRY(dev_alloc(&ix->dev.planner, ABF_PLANNER_PARAMS));
+    CUDA_TRY(cudaMemcpy(ix->dev.planner, h_params, sizeof(float) * ABF_PLANNER_PARAMS, cudaMemcpyHostToDevice));
+    return ABF_OK;
+    API_END
+}
+
+abf_status abf_planner_predict(abf_index* ix, const uint32_t* d_terms, const uint64_t* d_offsets, uint32_t n_q,
+                               float* d_pred, uint8_t* d_paths, void* stream) {
+    API_BEGIN
+    ABF_TRY(need_device(ix));
+    if (!ix->dev.planner) return fail(ABF_ERR_STATE, "no planner parameters installed (abf_planner_set)");
+    if (n_q && (!d_terms || !d_offsets)) return fail(ABF_ERR_INVALID, "abf_planner_predict: null pointer");
+    CUDA_TRY(cudaSetDevice(ix->device));
+    CUDA_TRY(abf::launch_planner(abf::view_of(ix), ix->dev.planner, d_terms, d_offsets, n_q, ix->tuning.heavy_min_len,
+                                 ix->n_postings, nullptr, d_pred, d_paths, static_cast<cudaStream_t>(stream)));
+    return ABF_OK;
+    API_END
+}
+
+abf_status abf_mlp_forward(const float* d_params, const float* d_x, uint32_t n, float* d_y, void* stream) {
+    API_BEGIN
+    if (!d_params || (n && (!d_x || !d_y))) return fail(ABF_ERR_INVALID, "abf_mlp_forward: null pointer");
+    CUDA_TRY(abf::launch_mlp_forward(d_params, d_x, n, d_y, static_cast<cudaStream_t>(stream)));
+    return ABF_OK;
+    API_END
+}
+
+abf_status abf_mlp_grad(const float* d_params, const float* d_x, const float* d_t, const float* d_mask, uint32_t n,
+                        float* d_grad, float* d_loss, void* stream) {
+    API_BEGIN
+    if (!d_params || !d_grad || !d_loss || (n && (!d_x || !d_t || !d_mask)))
+        return fail(ABF_ERR_INVALID, "abf_mlp_grad: null pointer");
+    CUDA_TRY(abf::launch_mlp_grad(d_params, d_x, d_t, d_mask, n, d_grad, d_loss, static_cast<cudaStream_t>(stream)));
+    return ABF_OK;
+    API_END
+}
+
+abf_status abf_mlp_adam(float* d_params, const float* d_grad, float* d_m, float* d_v, uint32_t step, float lr,
+                        float beta1, float beta2, float eps, void* stream) {
+    API_BEGIN
+    if (!d_params || !d_grad || !d_m || !d_v) return fail(ABF_ERR_INVALID, "abf_mlp_adam: null pointer");
+    CUDA_TRY(abf::launch_adam(d_params, d_grad, d_m, d_v, step, lr, beta1, beta2, eps,
+                              static_cast<cudaStream_t>(stream)));
+    return ABF_OK;
+    API_END
 }
 
 abf_status abf_index_list_flags(const abf_index* ix, uint32_t* h_out, uint32_t n) {

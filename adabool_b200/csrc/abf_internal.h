@@ -104,6 +104,8 @@ struct DeviceIndex {
     uint32_t* dense = nullptr;
     uint32_t* term_dir = nullptr;
     uint32_t* dir = nullptr;
+    uint32_t* term_cbytes = nullptr;  // compressed bytes per term (planner feature)
+    float* planner = nullptr;         // planner parameters (ABF_PLANNER_PARAMS) or null
     uint64_t bytes = 0;
 };
 
@@ -120,6 +122,7 @@ struct IndexView {
     const uint32_t* dense;
     const uint32_t* term_dir;
     const uint32_t* dir;
+    const uint32_t* term_cbytes;
     uint64_t dense_stride;
     uint32_t dir_n;
     uint32_t n_terms;

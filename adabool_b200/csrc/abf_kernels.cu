@@ -15,6 +15,7 @@
 #include "abf_kernels.cuh"
 
 #include <algorithm>
+#include <atomic>
 
 namespace abf {
 
@@ -947,6 +948,7 @@ IndexView view_of(const abf_index* ix) {
     v.dense = ix->dev.dense;
     v.term_dir = ix->dev.term_dir;
     v.dir = ix->dev.dir;
+    v.term_cbytes = ix->dev.term_cbytes;
     v.dense_stride = ix->derived.dense_stride;
     v.dir_n = ix->derived.dir_n;
     v.n_terms = ix->n_terms;
@@ -986,9 +988,19 @@ template <int W, int NW>
 static cudaError_t tile_launch(const IndexView& v, const TileArgs& a, int grid, cudaStream_t s) {
     constexpr int smem = W * 4;
     if (smem > 48 * 1024) {
-        // opt in to more than 48 KB of dynamic shared memory (per device)
-        cudaError_t e = cudaFuncSetAttribute(tile_union_kernel<W, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        // opt in to more than 48 KB of dynamic shared memory, once per device
+        // (so that later launches, also under stream capture, make no
+        // host-side attribute call)
+        static std::atomic<uint64_t> done{0};
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
         if (e != cudaSuccess) return e;
+        const uint64_t bit = 1ull << (dev & 63);
+        if (!(done.load() & bit)) {
+            e = cudaFuncSetAttribute(tile_union_kernel<W, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            if (e != cudaSuccess) return e;
+            done.fetch_or(bit);
+        }
     }
     tile_union_kernel<W, NW><<<grid, NW * 32, smem, s>>>(v, a);
     return cudaGetLastError();

@@ -147,6 +147,16 @@ cudaError_t launch_scatter(const IndexView& v, const ScatterArgs& a, const abf_t
                            cudaStream_t s);
 cudaError_t launch_probe(const IndexView& v, const ProbeArgs& a, const abf_tuning& t, int sm_count,
                          cudaStream_t s);
+// planner (abf_planner.cu)
+cudaError_t launch_planner(const IndexView& v, const float* params, const uint32_t* terms, const uint64_t* q_off,
+                           uint32_t n_q, uint32_t hybrid_min, uint64_t n_postings, float* feat, float* pred,
+                           uint8_t* paths, cudaStream_t s);
+cudaError_t launch_mlp_forward(const float* p, const float* x, uint32_t n, float* y, cudaStream_t s);
+cudaError_t launch_mlp_grad(const float* p, const float* x, const float* t, const float* mask, uint32_t n, float* g,
+                            float* loss2, cudaStream_t s);
+cudaError_t launch_adam(float* p, const float* g, float* m, float* v, uint32_t step, float lr, float b1, float b2,
+                        float eps, cudaStream_t s);
+
 cudaError_t launch_compact_count(const CompactArgs& a, int sm_count, cudaStream_t s);
 cudaError_t launch_compact_scan(const CompactArgs& a, cudaStream_t s);
 cudaError_t launch_compact_write(const CompactArgs& a, int sm_count, cudaStream_t s);

@@ -203,6 +203,7 @@ class Index:
 
     def profile(self, on: bool = True):
         check(lib().abf_profile_enable(self._h, 1 if on else 0))
+        self._profiling = bool(on)
 
     def profile_read(self) -> dict:
         """{kernel: (launches, total_ms)} since the last read (synchronises)."""

@@ -283,6 +283,45 @@ abf_status abf_query(abf_index* index, const uint32_t* terms, uint32_t n_terms, 
                      uint64_t* d_count, void* stream);
 
 /* ------------------------------------------------------------------ */
+/* Learned path planner (no reference counterpart: the reference runs  */
+/* both paths on every query and has no selection rule)                */
+/* ------------------------------------------------------------------ */
+/* Per query, 16 features (term count, sum / max / mean / spread of list
+ * lengths, compressed bytes, estimated output density, dense-list and
+ * short-list counts, batch position and size, ...) feed an MLP
+ * 16 -> 64 -> 64 -> 3 (ReLU, FP32) that predicts log(microseconds) of the
+ * PROBE, UNION and HYBRID paths; the cheapest is taken. Parameter block
+ * (ABF_PLANNER_PARAMS floats): mu[16], sd[16] (feature standardisation),
+ * W1[64][16], b1[64], W2[64][64], b2[64], W3[3][64], b3[3]. */
+#define ABF_PLANNER_FEATURES 16
+#define ABF_PLANNER_HIDDEN 64
+#define ABF_PLANNER_OUTPUTS 3
+#define ABF_PLANNER_PARAMS (2 * 16 + 64 * 16 + 64 + 64 * 64 + 64 + 3 * 64 + 3)
+
+/* Raw (unstandardised) features of a batch: n_queries x 16 floats. */
+abf_status abf_planner_features(abf_index* index, const uint32_t* d_terms, const uint64_t* d_offsets,
+                                uint32_t n_queries, float* d_features, void* stream);
+/* Installs planner parameters (host array) on the index; NULL removes
+ * them. With parameters installed, ABF_PATH_AUTO queries of abf_batch_run
+ * and abf_query take the planner's choice instead of the fixed rule. */
+abf_status abf_planner_set(abf_index* index, const float* h_params);
+/* The fused feature + MLP kernel on its own: predictions (n x 3, may be
+ * NULL) and chosen abf_path per query (may be NULL). */
+abf_status abf_planner_predict(abf_index* index, const uint32_t* d_terms, const uint64_t* d_offsets,
+                               uint32_t n_queries, float* d_pred, uint8_t* d_paths, void* stream);
+
+/* Training kernels of the MLP on standardised features x (n x 16):
+ * forward (y: n x 3), mean-squared-error gradient over the entries where
+ * mask is non-zero (grad in the parameter layout, overwritten; d_loss
+ * points to 2 floats: the loss and the number of entries counted), and one
+ * Adam step. The mu/sd entries are never updated. */
+abf_status abf_mlp_forward(const float* d_params, const float* d_x, uint32_t n, float* d_y, void* stream);
+abf_status abf_mlp_grad(const float* d_params, const float* d_x, const float* d_t, const float* d_mask, uint32_t n,
+                        float* d_grad, float* d_loss, void* stream);
+abf_status abf_mlp_adam(float* d_params, const float* d_grad, float* d_m, float* d_v, uint32_t step, float lr,
+                        float beta1, float beta2, float eps, void* stream);
+
+/* ------------------------------------------------------------------ */
 /* Measurement                                                         */
 /* ------------------------------------------------------------------ */
 

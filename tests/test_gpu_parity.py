@@ -155,6 +155,37 @@ def test_dense_div_rebuild(small, variant):
         ix.set_dense_div(128 if variant == "ix" else None)
 
 
+def test_graph_executor_replays_bit_exact(small):
+    """One graph launch per batch: two different batches replayed through the
+    same captured graph (padded with empty queries) match the oracle."""
+    torch = _torch()
+    from adabool_b200.executor import GraphBatchExecutor
+    ix, n_words = small["ix"], small["n_words"]
+    qs = small["qs"]
+    max_t = sum(q.size for q in qs) + 8
+    cap = sum(expected(small["off"], small["ads"], q, n_words)[0].size for q in qs) + 8
+    ex = GraphBatchExecutor(ix, len(qs) + 3, max_t, path=ab.PATH_HYBRID, with_ids=True, ids_capacity=cap,
+                            per_query_paths=True).capture()
+    rng = np.random.default_rng(11)
+    for order in (np.arange(len(qs)), rng.permutation(len(qs))[:len(qs) - 5]):
+        batch = [qs[i] for i in order]
+        qoff = np.zeros(len(batch) + 1, np.uint64)
+        qoff[1:] = np.cumsum([q.size for q in batch])
+        flat = np.concatenate(batch).astype(np.uint32)
+        paths = rng.choice([1, 2, 3, 4], size=len(batch)).astype(np.uint8)
+        ex.set_batch(qoff, flat, paths)
+        ex.replay().synchronize()
+        got = ex.bitmaps.cpu().numpy().view(np.uint32)
+        idoff = ex.d_id_off.cpu().numpy()
+        ids = ex.d_ids.cpu().numpy().view(np.uint32)
+        for i, q in enumerate(batch):
+            e_ids, e_bm = expected(small["off"], small["ads"], q, n_words)
+            assert np.array_equal(got[i, :n_words], e_bm), (i, paths[i])
+            assert np.array_equal(ids[idoff[i]:idoff[i + 1]], e_ids)
+        for i in range(len(batch), ex.max_q):  # padding queries are empty
+            assert not got[i, :n_words].any()
+
+
 def test_reference_api_or_semantics(small):
     """Prepare + ListUnion_* OR into the caller's buffer like the reference."""
     torch = _torch()
