@@ -872,7 +872,7 @@ abf_status abf_set_tuning(abf_index* ix, const abf_tuning* t) {
         return fail(ABF_ERR_INVALID, "probe_chunk_blocks must be a positive multiple of 128");
     if (t->scatter_blocks_per_warp == 0 || t->ctas_per_sm == 0 || t->ctas_per_sm > 32)
         return fail(ABF_ERR_INVALID, "scatter_blocks_per_warp and ctas_per_sm (<= 32) must be positive");
-    if (t->probe_cap > 4096) return fail(ABF_ERR_INVALID, "probe_cap above 4096");
+    if (t->probe_cap > 65536) return fail(ABF_ERR_INVALID, "probe_cap above 65536");
     ix->tuning = *t;
     return ABF_OK;
 }

@@ -93,9 +93,11 @@ class GraphBatchExecutor:
         self._n_set = n_queries
 
     def replay(self):
+        """Launches the graph on the executor's stream (after set_batch's copies)."""
         if self.graph is None:
             self.capture()
-        self.graph.replay()
+        with self.torch.cuda.stream(self.stream):
+            self.graph.replay()
         return self
 
     def synchronize(self):

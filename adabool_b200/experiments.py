@@ -1,0 +1,164 @@
+"""Measurements beyond the default bench step: the batched graph executor on
+config c2 and the learned planner on it (config c3), against the plain
+per-query fixed-threshold path. Run through ``bench.py --mode planner``.
+
+c2: 16,384 queries (lognormal term counts, median 40, sigma 2, [1, 20000]) on
+    c1's index, one CUDA-graph launch per batch, bitmaps packed per query.
+c3: the planner trained on ~200k timing samples (each of 66,667 fresh seeded
+    queries timed alone on PROBE, UNION and HYBRID), judged by regret against
+    the per-query best path and by batch speed against the fixed rule.
+"""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+
+from . import _native as N
+from . import planner as P
+from . import workload as W
+from .executor import GraphBatchExecutor
+from .index import Index
+
+
+def _chunked_features(ix, qoff, qt, chunk, device):
+    """Features computed in batches of `chunk` queries (the inference batch
+    size), so batch-position features mean the same at training time."""
+    out = []
+    for a in range(0, qoff.size - 1, chunk):
+        b = min(qoff.size - 1, a + chunk)
+        out.append(P.features(ix, (qoff[a:b + 1] - qoff[a]).astype(np.uint64), qt[qoff[a]:qoff[b]], device))
+    return np.concatenate(out)
+
+
+def _time_replays(ex, reps):
+    torch = ex.torch
+    ex.replay()
+    ex.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(ex.stream)
+    for _ in range(reps):
+        ex.replay()
+    e1.record(ex.stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def planner_experiment(n_train: int = 66_667, batch_config: str = "c2", reps: int = 3, device: int = 0,
+                       per_query_sample: int = 2048, verbose: bool = False) -> dict:
+    import torch
+    t_start = time.time()
+    cfg = W.CONFIGS[batch_config]
+    L = cfg.lists
+    off, ads = W.gen_lists(L)
+    lens = np.diff(off).astype(np.uint32)
+    ix = Index.from_csr(off, ads, L.n_terms, L.n_ads, device=device)
+    del off, ads
+    # HYBRID merges per tile every list of at least n_ads/1024 postings (UNION
+    # merges only the dense-bitmap lists), so the three paths differ
+    B = cfg.queries.n_queries
+    # probe slots for a whole batch, so PROBE labels really run the probe
+    ix.set_tuning(heavy_min_len=max(128, L.n_ads // 1024), probe_cap=B)
+    # --- training labels on fresh queries ---
+    tq = W.QueriesSpec(n_train, cfg.queries.kind, cfg.queries.median, cfg.queries.sigma, cfg.queries.lo,
+                       cfg.queries.hi, seed=cfg.queries.seed + 7919)
+    tqoff, tqt = W.gen_queries(tq, lens)
+    t0 = time.time()
+    t_iso = P.collect_labels(ix, tqoff, tqt, device=device, verbose=verbose)
+    t_lab = P.collect_labels_batched(ix, tqoff, tqt, t_iso, group=B, device=device)
+    torch.cuda.empty_cache()
+    label_s = time.time() - t0
+    Xtr = _chunked_features(ix, tqoff, tqt, B, device)
+    t0 = time.time()
+    tr = P.train(Xtr, np.log(t_lab), epochs=120, batch=8192, lr=2e-3, device=device, verbose=verbose)
+    train_s = time.time() - t0
+    frac_tr = P.touched_fraction(ix, tqoff, tqt)
+    tau = P.calibrate_tau(frac_tr, t_lab)
+    # --- evaluation batch ---
+    qoff, qt = W.gen_queries(cfg.queries, lens)
+    n = qoff.size - 1
+    e_iso = P.collect_labels(ix, qoff, qt, device=device)
+    e_lab = P.collect_labels_batched(ix, qoff, qt, e_iso, group=B, device=device)
+    torch.cuda.empty_cache()
+    Xev = _chunked_features(ix, qoff, qt, B, device)
+    choice_pl = P.mlp_predict(tr.params, Xev, device).argmin(1)
+    frac = P.touched_fraction(ix, qoff, qt)
+    choice_fx = np.where(frac > tau, 0, 1)
+    regret = {"planner": P.evaluate(e_lab, choice_pl), "fixed_rule": P.evaluate(e_lab, choice_fx),
+              "always_probe": P.evaluate(e_lab, np.zeros(n, int)), "always_union": P.evaluate(e_lab, np.ones(n, int)),
+              "always_hybrid": P.evaluate(e_lab, np.full(n, 2)),
+              "planner_on_isolated_labels": P.evaluate(e_iso, choice_pl),
+              "fixed_rule_on_isolated_labels": P.evaluate(e_iso, choice_fx)}
+    paths_of = np.array(N.PLANNER_PATHS, np.uint8)
+    # --- batch throughput: one graph launch per batch of B queries ---
+    ex = GraphBatchExecutor(ix, n, int(qoff[-1]), path=N.PATH_HYBRID, per_query_paths=True, device=device)
+    ex.capture()
+    batch = {}
+    ref_bm = None
+    mism = 0
+    for name, ch in (("fixed_rule", choice_fx), ("oracle_best", e_lab.argmin(1)), ("always_union", np.ones(n, int)),
+                     ("always_hybrid", np.full(n, 2))):
+        ex.set_batch(qoff, qt, paths_of[ch])
+        ms = _time_replays(ex, reps)
+        batch[name] = {"ms": ms, "queries_per_s": n / (ms / 1e3)}
+        if ref_bm is None:
+            ref_bm = ex.bitmaps.clone()
+        else:
+            mism += int(not torch.equal(ref_bm, ex.bitmaps))
+    del ex
+    torch.cuda.empty_cache()
+    P.install(ix, tr.params)
+    exa = GraphBatchExecutor(ix, n, int(qoff[-1]), path=N.PATH_AUTO, per_query_paths=False, device=device)
+    exa.capture()
+    exa.set_batch(qoff, qt)
+    ms = _time_replays(exa, reps)
+    batch["planner"] = {"ms": ms, "queries_per_s": n / (ms / 1e3), "note": "planner kernel inside the graph"}
+    mism += int(not torch.equal(ref_bm, exa.bitmaps))
+    planner_bm = exa.bitmaps
+    # --- plain per-query fixed-threshold path: each query alone, one call per query ---
+    m = min(per_query_sample, n)
+    ws = ix.workspace(1, int(qoff[-1]))
+    stride = (ix.n_words + 3) // 4 * 4
+    bm1 = torch.empty(stride, dtype=torch.int32, device=device)
+    dt, do = P.device_batch(qoff, qt, device)
+    s = torch.cuda.Stream(device=device)
+    import ctypes as C
+    Lb = N.lib()
+
+    def one(i):
+        b = N.Batch(N.ptr(dt), C.c_void_p(do.data_ptr() + 8 * i), 1, None, int(paths_of[choice_fx[i]]), N.ptr(bm1),
+                    stride, None, 0, None)
+        N.check(Lb.abf_batch_run(ix.handle, ws.handle, C.byref(b), N.stream_ptr(s)))
+
+    for i in range(min(m, 16)):
+        one(i)
+    s.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for i in range(m):
+        one(i)
+    e1.record(s)
+    e1.synchronize()
+    pq_ms = e0.elapsed_time(e1)
+    for i in range(0, m, max(1, m // 32)):  # per-query results equal the batch rows
+        one(i)
+        s.synchronize()
+        mism += int(not torch.equal(bm1[:ix.n_words], planner_bm[i, :ix.n_words]))
+    per_query = {"queries": m, "ms": pq_ms, "queries_per_s": m / (pq_ms / 1e3),
+                 "note": "abf_batch_run with one query per call, fixed-rule path, back to back on one stream"}
+    P.uninstall(ix)
+    return {
+        "batch_config": batch_config, "n_queries": n, "terms": int(qoff[-1]),
+        "train": {"queries": n_train, "samples": int(t_lab.size), "label_seconds": round(label_s, 1),
+                  "train_seconds": round(train_s, 1), "train_mse": tr.train_loss, "val_mse": tr.val_loss,
+                  "epochs": tr.epochs},
+        "fixed_rule_tau": tau, "regret": regret, "batch": batch, "per_query_fixed": per_query,
+        "speedup_planner_batch_over_per_query_fixed": batch["planner"]["queries_per_s"] / per_query["queries_per_s"],
+        "speedup_planner_over_fixed_rule_batch": batch["planner"]["queries_per_s"] / batch["fixed_rule"]["queries_per_s"],
+        "bitmap_mismatches_across_choices": mism,
+        "path_share": {"planner": np.bincount(choice_pl, minlength=3).tolist(),
+                       "fixed_rule": np.bincount(choice_fx, minlength=3).tolist(),
+                       "best": np.bincount(e_lab.argmin(1), minlength=3).tolist()},
+        "tuning": dict(ix.tuning.as_dict(), dense_div=ix.dense_div),
+        "seconds": round(time.time() - t_start, 1), "params": tr.params,
+    }

@@ -120,6 +120,44 @@ def collect_labels(index, q_off: np.ndarray, q_terms: np.ndarray, paths=PATHS, d
     return out
 
 
+def collect_labels_batched(index, q_off: np.ndarray, q_terms: np.ndarray, iso: np.ndarray, group: int = 512,
+                           paths=PATHS, device: int = 0) -> np.ndarray:
+    """Per-query labels in batch context: the queries are cut into groups of
+    `group` (enough that the group's bitmaps do not fit in L2, as in a large
+    batch), every group runs once per path as one batch with all its queries
+    on that path, and each query's isolated time `iso` (n x paths) is scaled
+    so the group's labels add up to the measured batch time of that path."""
+    torch = _torch()
+    n = q_off.size - 1
+    dt, do = device_batch(q_off, q_terms, device)
+    ws = index.workspace(group, max(int(q_off[-1]), 1))
+    stride = (index.n_words + 3) // 4 * 4
+    bms = torch.empty((group, stride), dtype=torch.int32, device=device)
+    s = torch.cuda.Stream(device=device)
+    L = lib()
+    out = np.zeros_like(iso)
+
+    def run(a, b, p):
+        bt = N.Batch(ptr(dt), C.c_void_p(do.data_ptr() + 8 * a), b - a, None, p, ptr(bms), stride, None, 0, None)
+        check(L.abf_batch_run(index.handle, ws.handle, C.byref(bt), stream_ptr(s)))
+
+    run(0, min(n, group), PATHS[1])
+    s.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for a in range(0, n, group):
+        b = min(n, a + group)
+        for j, p in enumerate(paths):
+            e0.record(s)
+            run(a, b, p)
+            e1.record(s)
+            e1.synchronize()
+            t_us = e0.elapsed_time(e1) * 1e3
+            w = iso[a:b, j]
+            out[a:b, j] = w * (t_us / max(w.sum(), 1e-9))
+    ws.free()
+    return out
+
+
 @dataclass
 class TrainResult:
     params: np.ndarray

@@ -65,6 +65,10 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--out", default="", help="also append the JSON line to this file")
+    p.add_argument("--mode", default="step", choices=["step", "planner"],
+                   help="step: the default benchmark; planner: configs c2/c3 (graph executor, learned planner)")
+    p.add_argument("--planner-out", default="", help="planner mode: save the trained parameters (.npy)")
+    p.add_argument("--train-queries", type=int, default=66_667)
     return p.parse_args()
 
 
@@ -504,6 +508,20 @@ def dist_max(x: float, world: int) -> float:
 
 def main():
     args = parse()
+    if args.mode == "planner" and args.impl == "ours":
+        from adabool_b200 import experiments as X
+        from adabool_b200 import planner as P
+        r = X.planner_experiment(n_train=args.train_queries, verbose=True)
+        params = r.pop("params")
+        if args.planner_out:
+            P.save(params, args.planner_out, {k: r[k] for k in ("fixed_rule_tau", "tuning", "train")})
+        r["metric"] = METRIC
+        line = json.dumps(r)
+        print(line, flush=True)
+        if args.out:
+            with open(args.out, "a") as f:
+                f.write(line + "\n")
+        return 0
     if args.impl == "reference":
         if int(os.environ.get("RANK", "0")) != 0:
             return 0

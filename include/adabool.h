@@ -146,7 +146,7 @@ typedef struct abf_tuning {
     uint32_t probe_chunk_blocks; /* blocks per CTA in the bitmap-probe scan */
     uint32_t scatter_blocks_per_warp; /* consecutive blocks a union warp takes */
     uint32_t ctas_per_sm;     /* grid = SMs x this, for the persistent kernels */
-    uint32_t probe_cap;       /* queries of one batch that may take the probe path */
+    uint32_t probe_cap;       /* queries of one batch that may take the probe path (<= 65536) */
     float probe_min_fraction; /* fixed rule (ABF_PATH_AUTO without a planner): probe
                                  when the query's lists hold more than this fraction
                                  of all blocks, else list-union */
