@@ -82,6 +82,40 @@ class GenQueriesParams(C.Structure):
                 ("n_threads", C.c_int)]
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("budget_bytes", C.c_uint64), ("window_us", C.c_uint32), ("max_batch_queries", C.c_uint32),
+                ("max_batch_terms", C.c_uint64), ("n_streams", C.c_uint32), ("path", C.c_int),
+                ("outputs", C.c_uint32)]
+
+
+SERVE_BITMAPS = 1
+SERVE_IDS = 2
+
+
+class ServerResult(C.Structure):
+    _fields_ = [("ticket", C.c_uint64), ("tag", C.c_uint64), ("status", C.c_int32), ("path", C.c_uint32),
+                ("d_bitmap", vp), ("d_ids", vp), ("n_ids", C.c_uint64), ("t_arrival_ns", C.c_uint64),
+                ("t_launch_ns", C.c_uint64), ("t_done_ns", C.c_uint64), ("batch_queries", C.c_uint32),
+                ("pad_", C.c_uint32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(f, C.c_uint64) for f in ("submitted", "completed", "released", "rejected", "batches",
+                                          "failed_batches", "waiting", "in_flight_batches", "pool_bytes",
+                                          "reserved_bytes", "peak_reserved_bytes", "admission_waits")] + \
+               [("path_queries", C.c_uint64 * 5), ("max_batch_queries_seen", C.c_uint64)]
+
+    def as_dict(self):
+        d = {f: getattr(self, f) for f, _ in self._fields_}
+        d["path_queries"] = list(self.path_queries)
+        return d
+
+
+class TraceStats(C.Structure):
+    _fields_ = [("seconds", C.c_double), ("completed", C.c_uint64), ("rejected", C.c_uint64),
+                ("failed", C.c_uint64)]
+
+
 # (name, argtypes) of every exported entry point; restype is abf_status
 # (c_int) unless listed in _RESTYPES.
 PROTOTYPES = {
@@ -123,6 +157,15 @@ PROTOTYPES = {
     "abf_index_list_flags": [vp, u32p, C.c_uint32],
     "abf_profile_enable": [vp, C.c_int],
     "abf_profile_read": [vp, vp, C.c_uint32, u32p],
+    "abf_clock_ns": [],
+    "abf_server_default_opts": [C.POINTER(ServerOpts)],
+    "abf_server_create": [vp, C.POINTER(ServerOpts), C.POINTER(vp)],
+    "abf_server_submit": [vp, u32p, C.c_uint32, C.c_uint64, C.c_uint64, u64p],
+    "abf_server_poll": [vp, C.POINTER(ServerResult), C.c_uint32, C.c_uint32, u32p],
+    "abf_server_release": [vp, C.c_uint64],
+    "abf_server_get_stats": [vp, C.POINTER(ServerStats)],
+    "abf_server_destroy": [vp],
+    "abf_server_run_trace": [vp, u32p, u64p, C.c_uint32, u64p, C.c_double, u64p, u64p, u8p, C.POINTER(TraceStats)],
     "abf_last_error_string": [],
     "abf_status_string": [C.c_int],
     "abf_abi_version": [],
@@ -134,7 +177,7 @@ PROTOTYPES = {
     "abf_gen_queries_fill": [C.POINTER(GenQueriesParams), u32p, C.c_uint32, u64p, u32p],
 }
 _RESTYPES = {"abf_last_error_string": C.c_char_p, "abf_status_string": C.c_char_p,
-             "abf_abi_version": C.c_uint32, "abf_launch_count": C.c_uint64}
+             "abf_abi_version": C.c_uint32, "abf_launch_count": C.c_uint64, "abf_clock_ns": C.c_uint64}
 
 _lib = None
 

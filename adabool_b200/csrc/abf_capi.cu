@@ -1069,6 +1069,15 @@ abf_status abf_workspace_create(abf_index* ix, uint32_t max_queries, uint64_t ma
     API_END
 }
 
+}  // extern "C"
+
+namespace abf {
+const uint8_t* ws_paths(const abf_workspace* w) { return w->path_out; }
+uint32_t* ws_err(abf_workspace* w) { return w->err; }
+}  // namespace abf
+
+extern "C" {
+
 abf_status abf_workspace_free(abf_workspace* w) {
     API_BEGIN
     if (!w) return ABF_OK;

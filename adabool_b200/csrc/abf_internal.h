@@ -181,4 +181,9 @@ int resolve_threads(int n);
 // dense bitmaps and block directory of a host index (abf_build.cpp)
 void derive_tables(const HostIndex& h, uint32_t dense_div, int n_threads, DerivedHost* out);
 
+// device arrays of a workspace that the serving loop reads back after a
+// batch (abf_capi.cu): the path each query ran on and the error flag
+const uint8_t* ws_paths(const abf_workspace* w);
+uint32_t* ws_err(abf_workspace* w);
+
 }  // namespace abf

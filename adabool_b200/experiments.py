@@ -162,3 +162,106 @@ def planner_experiment(n_train: int = 66_667, batch_config: str = "c2", reps: in
         "tuning": dict(ix.tuning.as_dict(), dense_div=ix.dense_div),
         "seconds": round(time.time() - t_start, 1), "params": tr.params,
     }
+
+
+def _train_for_groups(ix, qoff, qt, iso, groups, device, verbose=False):
+    """Planner trained on labels measured in batches of several sizes, each
+    with its features computed in batches of the same size."""
+    X, Y = [], []
+    for g in groups:
+        Y.append(P.collect_labels_batched(ix, qoff, qt, iso, group=g, device=device))
+        X.append(_chunked_features(ix, qoff, qt, g, device))
+    X, Y = np.concatenate(X), np.concatenate(Y)
+    tr = P.train(X, np.log(Y), epochs=120, batch=8192, lr=2e-3, device=device, verbose=verbose)
+    return tr, X, Y
+
+
+def serving_experiment(rates=(20_000, 50_000, 100_000, 200_000), offered_seconds: float = 0.5,
+                       min_queries: int = 4000, n_train: int = 20_000, label_groups=(32, 256, 1024),
+                       budget_bytes: int = 40 << 30, window_us: int = 200, max_batch_queries: int = 1024,
+                       n_streams: int = 2, device: int = 0, planner_params=None, verbose: bool = False) -> dict:
+    """Config c4: open-loop Poisson arrivals on c1's index, served by the
+    batching server with the learned planner, by the same server with the
+    fixed threshold rule, and by the plain per-query fixed-rule path (one
+    query per abf_batch_run, one stream); throughput and latency
+    percentiles per arrival rate."""
+    import torch
+    from .server import Server, latency_summary, poisson_arrivals
+    t_start = time.time()
+    cfg = W.CONFIGS["c4"]
+    L = cfg.lists
+    off, ads = W.gen_lists(L)
+    lens = np.diff(off).astype(np.uint32)
+    ix = Index.from_csr(off, ads, L.n_terms, L.n_ads, device=device)
+    del off, ads
+    ix.set_tuning(heavy_min_len=max(128, L.n_ads // 1024), probe_cap=max_batch_queries)
+    # --- planner and fixed-rule threshold from batched timing labels ---
+    tq = W.QueriesSpec(n_train, cfg.queries.kind, cfg.queries.median, cfg.queries.sigma, cfg.queries.lo,
+                       cfg.queries.hi, seed=cfg.queries.seed + 7919)
+    tqoff, tqt = W.gen_queries(tq, lens)
+    t0 = time.time()
+    iso = P.collect_labels(ix, tqoff, tqt, device=device, verbose=verbose)
+    tr, _, Y = _train_for_groups(ix, tqoff, tqt, iso, label_groups, device, verbose)
+    if planner_params is not None:
+        tr.params = np.asarray(planner_params, np.float32)
+    frac = np.tile(P.touched_fraction(ix, tqoff, tqt), len(label_groups))
+    tau = P.calibrate_tau(frac, Y)
+    ix.set_tuning(probe_min_fraction=tau)
+    train_s = time.time() - t0
+    torch.cuda.empty_cache()
+    # --- arrivals ---
+    n_max = max(int(max(rates) * offered_seconds), min_queries)
+    qspec = W.QueriesSpec(n_max, cfg.queries.kind, cfg.queries.median, cfg.queries.sigma, cfg.queries.lo,
+                          cfg.queries.hi, seed=cfg.queries.seed)
+    qoff, qt = W.gen_queries(qspec, lens)
+    servers = {
+        "planner_batched": dict(path=N.PATH_AUTO, planner=True, max_batch_queries=max_batch_queries,
+                                n_streams=n_streams, window_us=window_us),
+        "fixed_rule_batched": dict(path=N.PATH_AUTO, planner=False, max_batch_queries=max_batch_queries,
+                                   n_streams=n_streams, window_us=window_us),
+        "per_query_fixed_rule": dict(path=N.PATH_AUTO, planner=False, max_batch_queries=1, n_streams=1,
+                                     window_us=0),
+    }
+    runs = []
+    for rate in rates:
+        n = max(int(rate * offered_seconds), min_queries)
+        arr = poisson_arrivals(rate, n, seed=int(rate))
+        sub_off = qoff[:n + 1]
+        sub_t = qt[:int(sub_off[-1])]
+        ref_ids = None
+        for name, sc in servers.items():
+            if sc["planner"]:
+                P.install(ix, tr.params)
+            else:
+                P.uninstall(ix)
+            with Server(ix, budget_bytes=budget_bytes, window_us=sc["window_us"],
+                        max_batch_queries=sc["max_batch_queries"], n_streams=sc["n_streams"],
+                        path=sc["path"]) as srv:
+                out = srv.run_trace(sub_off, sub_t, arr, timeout_s=600)
+                st = srv.stats()
+            mism = 0
+            if ref_ids is None:
+                ref_ids = out["n_ids"]
+            else:
+                mism = int((out["n_ids"] != ref_ids).sum())
+            rec = {"rate_qps": rate, "server": name, "queries": n, "completed": out["completed"],
+                   "rejected": out["rejected"], "failed": out["failed"], "seconds": out["seconds"],
+                   "throughput_qps": out["completed"] / max(out["seconds"], 1e-9),
+                   **latency_summary(out["latency_ns"]),
+                   "batches": st["batches"], "mean_batch": st["completed"] / max(st["batches"], 1),
+                   "max_batch": st["max_batch_queries_seen"], "admission_waits": st["admission_waits"],
+                   "peak_reserved_gb": st["peak_reserved_bytes"] / 1e9,
+                   "paths": {N.PATH_NAMES[p]: int(c) for p, c in enumerate(st["path_queries"]) if c},
+                   "id_count_mismatches_vs_first_server": mism}
+            if verbose:
+                print(rec, flush=True)
+            runs.append(rec)
+    P.uninstall(ix)
+    return {"config": "c4", "index": {"n_terms": L.n_terms, "n_ads": L.n_ads, "nnz": L.nnz},
+            "queries": {"median_terms": cfg.queries.median, "sigma": cfg.queries.sigma, "max_terms": cfg.queries.hi},
+            "budget_bytes": budget_bytes, "window_us": window_us, "max_batch_queries": max_batch_queries,
+            "n_streams": n_streams, "fixed_rule_tau": tau,
+            "planner_train": {"queries": n_train, "groups": list(label_groups), "samples": int(Y.shape[0]),
+                              "val_mse": tr.val_loss, "seconds": round(train_s, 1)},
+            "runs": runs, "tuning": dict(ix.tuning.as_dict(), dense_div=ix.dense_div),
+            "seconds": round(time.time() - t_start, 1), "params": tr.params}

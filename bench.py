@@ -65,8 +65,11 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--out", default="", help="also append the JSON line to this file")
-    p.add_argument("--mode", default="step", choices=["step", "planner"],
-                   help="step: the default benchmark; planner: configs c2/c3 (graph executor, learned planner)")
+    p.add_argument("--mode", default="step", choices=["step", "planner", "serve"],
+                   help="step: the default benchmark; planner: configs c2/c3 (graph executor, learned planner); "
+                        "serve: config c4 (Poisson arrivals through the serving loop)")
+    p.add_argument("--rates", default="20000,50000,100000,200000", help="serve mode: arrival rates (queries/s)")
+    p.add_argument("--offered-seconds", type=float, default=0.5, help="serve mode: arrivals per rate, in seconds")
     p.add_argument("--planner-out", default="", help="planner mode: save the trained parameters (.npy)")
     p.add_argument("--train-queries", type=int, default=66_667)
     return p.parse_args()
@@ -516,6 +519,19 @@ def main():
         if args.planner_out:
             P.save(params, args.planner_out, {k: r[k] for k in ("fixed_rule_tau", "tuning", "train")})
         r["metric"] = METRIC
+        line = json.dumps(r)
+        print(line, flush=True)
+        if args.out:
+            with open(args.out, "a") as f:
+                f.write(line + "\n")
+        return 0
+    if args.mode == "serve" and args.impl == "ours":
+        from adabool_b200 import experiments as X
+        rates = tuple(int(float(x)) for x in args.rates.split(","))
+        r = X.serving_experiment(rates=rates, offered_seconds=args.offered_seconds,
+                                 n_train=min(args.train_queries, 20_000), verbose=True)
+        r.pop("params")
+        r["metric"] = "serving throughput (queries/s) and p50/p99/p99.9 latency vs per-query fixed-rule path"
         line = json.dumps(r)
         print(line, flush=True)
         if args.out:

@@ -352,6 +352,111 @@ abf_status abf_profile_enable(abf_index* index, int on);
 abf_status abf_profile_read(abf_index* index, abf_kernel_time* out, uint32_t cap, uint32_t* n_out);
 
 /* ------------------------------------------------------------------ */
+/* Serving loop (no reference counterpart: the reference answers one    */
+/* query, or one batch of at most 32, per host call)                    */
+/* ------------------------------------------------------------------ */
+/* A server owns one host thread that batches submitted queries and runs
+ * each batch through abf_batch_run on one of n_streams streams, so the
+ * next batch is cut and launched while earlier ones run (continuous
+ * batching):
+ *   - admission: a batch takes one range of a device pool of budget_bytes,
+ *     allocated when the server is created: n x bitmap_stride_words x 4
+ *     bytes of bitmaps plus, with ABF_SERVE_IDS, 4 x min(n_ads, sum of the
+ *     query's list lengths) bytes of id room per query. Queries are cut
+ *     first-in first-out; the first one that does not fit the largest free
+ *     extent waits, with everything behind it, until results are released;
+ *   - batching: with nothing in flight, whatever waits is launched at once;
+ *     otherwise a free stream takes a batch once the oldest waiting query
+ *     has waited window_us, or max_batch_queries / max_batch_terms are
+ *     reached;
+ *   - results stay in the pool (bitmap and ascending ids, device memory)
+ *     until abf_server_release. When a batch completes, its id room is
+ *     trimmed to the ids written and, without ABF_SERVE_BITMAPS, its
+ *     bitmaps are freed. A batch's range is returned to the pool when the
+ *     last of its queries is released.
+ * Every query's result is the same whatever batch it runs in. Submit, poll
+ * and release may be called from any threads. Kernel timing
+ * (abf_profile_enable) must be off on the index while a server runs. */
+typedef struct abf_server abf_server;
+
+#define ABF_SERVE_BITMAPS 1u    /* keep each query's bitmap in its result */
+#define ABF_SERVE_IDS 2u        /* compute each query's ascending ids */
+
+typedef struct abf_server_opts {
+    uint64_t budget_bytes;       /* device pool for bitmaps and ids (default 40 GiB) */
+    uint32_t window_us;          /* longest wait of the oldest query before a cut (default 200) */
+    uint32_t max_batch_queries;  /* default 1024 */
+    uint64_t max_batch_terms;    /* default 2^22; also the longest query accepted */
+    uint32_t n_streams;          /* batches in flight, 1..8 (default 2) */
+    abf_path path;               /* path of every query; AUTO = installed planner, else fixed rule */
+    uint32_t outputs;            /* ABF_SERVE_BITMAPS | ABF_SERVE_IDS (default both) */
+} abf_server_opts;
+
+typedef struct abf_server_result {
+    uint64_t ticket;
+    uint64_t tag;                /* as given to abf_server_submit */
+    int32_t status;              /* ABF_OK, or the error of the query's batch */
+    uint32_t path;               /* abf_path the query ran on */
+    const uint32_t* d_bitmap;    /* (n_ads+31)/32 words, device; NULL without ABF_SERVE_BITMAPS */
+    const uint32_t* d_ids;       /* ascending ids, device; NULL without ABF_SERVE_IDS */
+    uint64_t n_ids;
+    uint64_t t_arrival_ns;       /* abf_clock_ns() times */
+    uint64_t t_launch_ns;
+    uint64_t t_done_ns;          /* when the server thread saw the batch complete */
+    uint32_t batch_queries;      /* size of the batch it ran in */
+    uint32_t pad_;
+} abf_server_result;
+
+typedef struct abf_server_stats {
+    uint64_t submitted, completed, released, rejected;
+    uint64_t batches, failed_batches;
+    uint64_t waiting, in_flight_batches;
+    uint64_t pool_bytes, reserved_bytes, peak_reserved_bytes;
+    uint64_t admission_waits;    /* cuts that left a waiting query behind for lack of pool
+                                    room, plus stretches with no room for the head query */
+    uint64_t path_queries[5];    /* queries per abf_path taken */
+    uint64_t max_batch_queries_seen;
+} abf_server_stats;
+
+/* Monotonic clock of the server, nanoseconds (CLOCK_MONOTONIC). */
+uint64_t abf_clock_ns(void);
+abf_status abf_server_default_opts(abf_server_opts* opts);
+/* The index must be on a device and outlive the server. */
+abf_status abf_server_create(abf_index* index, const abf_server_opts* opts, abf_server** out);
+/* Copies the terms; arrival_ns 0 = now. Term ids >= n_terms match
+ * nothing (as in abf_query). ABF_ERR_CAPACITY for a query longer than
+ * max_batch_terms or
+ * whose bitmap and id room exceed the whole pool; ABF_ERR_STATE once the
+ * server is being destroyed. */
+abf_status abf_server_submit(abf_server* server, const uint32_t* terms, uint32_t n_terms, uint64_t tag,
+                             uint64_t arrival_ns, uint64_t* ticket);
+/* Moves up to max_results finished queries into out, waiting up to
+ * timeout_us for the first one. */
+abf_status abf_server_poll(abf_server* server, abf_server_result* out, uint32_t max_results,
+                           uint32_t timeout_us, uint32_t* n_out);
+/* Frees a polled result (its device pointers become invalid). */
+abf_status abf_server_release(abf_server* server, uint64_t ticket);
+abf_status abf_server_get_stats(abf_server* server, abf_server_stats* out);
+/* Fails the queries still waiting, waits for the batches in flight and
+ * frees the pool (every result pointer becomes invalid). */
+abf_status abf_server_destroy(abf_server* server);
+
+/* Open-loop load: query i (terms[offsets[i] .. offsets[i+1])) is submitted
+ * at start + arrival_ns[i] (ascending) by a generator thread, with that
+ * time as its arrival; the calling thread polls and releases results as
+ * they come. Per query: latency_ns (t_done - arrival; UINT64_MAX when
+ * rejected or failed), and optionally n_ids and the path taken. Returns
+ * when every query is done, or ABF_ERR_TIMEOUT after timeout_s. */
+typedef struct abf_trace_stats {
+    double seconds;              /* first arrival to last completion */
+    uint64_t completed, rejected, failed;
+} abf_trace_stats;
+abf_status abf_server_run_trace(abf_server* server, const uint32_t* terms, const uint64_t* offsets,
+                                uint32_t n_queries, const uint64_t* arrival_ns, double timeout_s,
+                                uint64_t* h_latency_ns, uint64_t* h_n_ids, uint8_t* h_paths,
+                                abf_trace_stats* out);
+
+/* ------------------------------------------------------------------ */
 /* Misc                                                                */
 /* ------------------------------------------------------------------ */
 const char* abf_last_error_string(void);
