@@ -165,7 +165,8 @@ PROTOTYPES = {
     "abf_server_release": [vp, C.c_uint64],
     "abf_server_get_stats": [vp, C.POINTER(ServerStats)],
     "abf_server_destroy": [vp],
-    "abf_server_run_trace": [vp, u32p, u64p, C.c_uint32, u64p, C.c_double, u64p, u64p, u8p, C.POINTER(TraceStats)],
+    "abf_server_run_trace": [vp, u32p, u64p, C.c_uint32, u64p, C.c_double, u64p, u64p, u64p, u8p,
+                             C.POINTER(TraceStats)],
     "abf_last_error_string": [],
     "abf_status_string": [C.c_int],
     "abf_abi_version": [],

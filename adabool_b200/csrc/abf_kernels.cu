@@ -789,14 +789,16 @@ __global__ void __launch_bounds__(kScanNT) scan_kernel(const uint32_t* in, uint6
     if (tile == last_tile && tid == 0) out[n] = s_prefix + agg;
 }
 
-// One CTA per (bitmap, 2048-word chunk): the chunk is staged in shared
-// memory, its 64 units of 32 words are counted and scanned once, then every
-// warp expands its units on its own, one word at a time with one lane per
-// bit: the lanes holding set bits store their ids to consecutive output
+// One CTA per (bitmap, 2048-word chunk) at a time; each of its 8 warps owns
+// 8 consecutive units of 32 words, held in registers (lane l: word l of
+// each unit). One barrier per chunk exchanges the warps' id totals; then
+// every warp expands its units on its own, one word at a time with one lane
+// per bit: the lanes holding set bits store their ids to consecutive output
 // addresses (rank = popcount of the lower bits), so each store instruction
 // writes one contiguous run and no lane loops over bits.
 constexpr uint32_t kUnits = kCompactChunkWords / 32;
-static_assert(kUnits == 64, "the unit scan below covers 64 units with one warp");
+constexpr uint32_t kWarpUnits = kUnits / 8;
+static_assert(kUnits == 64, "8 warps x 8 units cover one chunk");
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
@@ -816,54 +818,73 @@ __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wa
 
 constexpr uint32_t kIdBuf = 1024 + 8;  // one unit's ids plus the 16-byte alignment head
 
+// Ids of one unit into dst[0 .. tot): lane l holds word l of the unit in v
+// and the ids of the lower lanes' words in ex; id0 = first id of the unit +
+// lane. Dense units walk all 32 words without bookkeeping; sparse ones
+// visit only the non-zero words.
+template <bool kDense, typename Store>
+__device__ __forceinline__ void expand_unit(uint32_t v, uint32_t ex, uint32_t id0, uint32_t lt, uint32_t mybit,
+                                            Store store) {
+    if (kDense) {
+#pragma unroll 8
+        for (uint32_t w = 0; w < 32u; ++w) {
+            const uint32_t word = __shfl_sync(kFull, v, w);
+            const uint32_t pos = __shfl_sync(kFull, ex, w);
+            if (word & mybit) store(pos + __popc(word & lt), id0 + w * 32u);
+        }
+    } else {
+        uint32_t nz = __ballot_sync(kFull, v != 0u);
+        while (nz) {
+            const uint32_t w = __ffs(nz) - 1u;
+            nz &= nz - 1u;
+            const uint32_t word = __shfl_sync(kFull, v, w);
+            const uint32_t pos = __shfl_sync(kFull, ex, w);
+            if (word & mybit) store(pos + __popc(word & lt), id0 + w * 32u);
+        }
+    }
+}
+
 __global__ void __launch_bounds__(256) write_ids_kernel(CompactArgs a) {
-    __shared__ __align__(16) uint32_t s_words[kCompactChunkWords];
-    __shared__ uint32_t s_unit[kUnits];
     __shared__ __align__(16) uint32_t s_buf[8][kIdBuf];
-    const uint32_t tid = threadIdx.x, lane = lane_id(), warp = warp_id();
-    const uint32_t lt = lanemask_lt();
+    __shared__ uint32_t s_wtot[2][8];  // per-warp id totals, double-buffered by chunk parity
+    const uint32_t lane = lane_id(), warp = warp_id();
+    const uint32_t lt = lanemask_lt(), mybit = 1u << lane;
     const bool ids16 = (reinterpret_cast<uintptr_t>(a.ids) & 15u) == 0;
     uint32_t* buf = s_buf[warp];
     const uint64_t n_words = (a.n_bits + 31) / 32;
     const uint64_t items = uint64_t(a.n_q) * a.n_chunks;
-    for (uint64_t item = blockIdx.x; item < items; item += gridDim.x) {
+    uint32_t parity = 0;
+    for (uint64_t item = blockIdx.x; item < items; item += gridDim.x, parity ^= 1u) {
         const uint32_t q = uint32_t(item / a.n_chunks);
         const uint32_t c = uint32_t(item - uint64_t(q) * a.n_chunks);
         const uint32_t* bm = a.bm + uint64_t(q) * a.stride;
         const uint64_t out = a.offsets[item];
-        if (c == 0 && tid == 0) {
+        if (c == 0 && threadIdx.x == 0) {
             if (a.id_offsets) a.id_offsets[q] = out;
             if (a.id_counts) a.id_counts[q] = a.offsets[item + a.n_chunks] - out;
             if (a.id_offsets && q == a.n_q - 1) a.id_offsets[a.n_q] = a.offsets[items];
         }
-        const uint64_t w0 = uint64_t(c) * kCompactChunkWords;
-        const uint32_t nwc = uint32_t(w0 + kCompactChunkWords < n_words ? kCompactChunkWords : n_words - w0);
-        for (uint32_t i = tid; i < kCompactChunkWords; i += 256)
-            s_words[i] = i < nwc ? masked_word(bm, w0 + i, a.n_bits) : 0u;
-        __syncthreads();
-        for (uint32_t u = warp; u < kUnits; u += 8) {
-            uint32_t s = __popc(s_words[u * 32u + lane]);
+        const uint64_t wbase = uint64_t(c) * kCompactChunkWords + uint64_t(warp) * (kWarpUnits * 32u);
+        uint32_t v[kWarpUnits], tot[kWarpUnits];
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(kFull, s, o);
-            if (lane == 0) s_unit[u] = s;
+        for (uint32_t k = 0; k < kWarpUnits; ++k) {
+            const uint64_t wi = wbase + k * 32u + lane;
+            v[k] = wi < n_words ? masked_word(bm, wi, a.n_bits) : 0u;
         }
-        __syncthreads();
-        if (warp == 0) {
-            const uint32_t v0 = s_unit[2 * lane], v1 = s_unit[2 * lane + 1];
-            uint32_t x = v0 + v1;
+        uint32_t wsum = 0;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t y = __shfl_up_sync(kFull, x, o);
-                if (lane >= uint32_t(o)) x += y;
-            }
-            const uint32_t ex = x - v0 - v1;
-            s_unit[2 * lane] = ex;
-            s_unit[2 * lane + 1] = ex + v0;
+        for (uint32_t k = 0; k < kWarpUnits; ++k) {
+            tot[k] = __reduce_add_sync(kFull, uint32_t(__popc(v[k])));
+            wsum += tot[k];
         }
+        if (lane == 0) s_wtot[parity][warp] = wsum;
         __syncthreads();
-        for (uint32_t u = warp; u < kUnits; u += 8) {
-            const uint32_t v = s_words[u * 32u + lane];
-            const uint32_t cnt = __popc(v);
+        uint64_t o0 = out + __reduce_add_sync(kFull, lane < warp ? s_wtot[parity][lane] : 0u);
+#pragma unroll
+        for (uint32_t k = 0; k < kWarpUnits; ++k) {
+            const uint32_t t = tot[k];
+            if (t == 0) continue;
+            const uint32_t cnt = __popc(v[k]);
             uint32_t x = cnt;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -871,28 +892,22 @@ __global__ void __launch_bounds__(256) write_ids_kernel(CompactArgs a) {
                 if (lane >= uint32_t(o)) x += y;
             }
             const uint32_t ex = x - cnt;
-            const uint64_t o0 = out + s_unit[u];
-            const uint32_t my_id = uint32_t((w0 + u * 32u) * 32u) + lane;
-            uint32_t nz = __ballot_sync(kFull, v != 0u);
+            const uint32_t id0 = uint32_t((wbase + k * 32u) * 32u) + lane;
             uint32_t* dst = a.ids + o0;
-            const uint32_t tot = __shfl_sync(kFull, x, 31);
-            if (ids16 && tot >= 64 && o0 + tot <= a.capacity) {
-                // dense unit: ids go to the warp's shared buffer at their
-                // 16-byte-aligned output position, the aligned middle leaves
+            if (ids16 && t >= 64 && o0 + t <= a.capacity) {
+                // the unit's ids go to the warp's shared buffer at their
+                // 16-byte-aligned output position; the aligned middle leaves
                 // by one bulk copy, the ragged ends by plain stores
                 const uint32_t head = uint32_t(o0 & 3u);
+                uint32_t* sb = buf + head;
                 if (lane == 0) bulk_wait_read_all();  // the previous unit's copy has read the buffer
                 __syncwarp();
-                while (nz) {
-                    const uint32_t w = __ffs(nz) - 1u;
-                    nz &= nz - 1u;
-                    const uint32_t word = __shfl_sync(kFull, v, w);
-                    const uint32_t pos = __shfl_sync(kFull, ex, w);
-                    if ((word >> lane) & 1u) buf[head + pos + __popc(word & lt)] = my_id + w * 32u;
-                }
+                auto st = [sb](uint32_t i, uint32_t id) { sb[i] = id; };
+                if (t >= 256u) expand_unit<true>(v[k], ex, id0, lt, mybit, st);
+                else expand_unit<false>(v[k], ex, id0, lt, mybit, st);
                 fence_proxy_async();  // these shared writes before the async-proxy read
                 __syncwarp();
-                const uint32_t end = head + tot;
+                const uint32_t end = head + t;
                 const uint32_t mid_hi = end & ~3u;
                 uint32_t* gbase = dst - head;  // 16-byte aligned
                 if (lane == 0 && mid_hi > 4u) {
@@ -901,28 +916,18 @@ __global__ void __launch_bounds__(256) write_ids_kernel(CompactArgs a) {
                 }
                 if (lane >= head && lane < 4u) gbase[lane] = buf[lane];
                 if (mid_hi + lane < end) gbase[mid_hi + lane] = buf[mid_hi + lane];
-            } else if (o0 + tot <= a.capacity) {  // whole unit fits: no per-id check
-                while (nz) {
-                    const uint32_t w = __ffs(nz) - 1u;
-                    nz &= nz - 1u;
-                    const uint32_t word = __shfl_sync(kFull, v, w);
-                    const uint32_t pos = __shfl_sync(kFull, ex, w);
-                    if ((word >> lane) & 1u) dst[pos + __popc(word & lt)] = my_id + w * 32u;
-                }
+            } else if (o0 + t <= a.capacity) {  // whole unit fits: no per-id check
+                expand_unit<false>(v[k], ex, id0, lt, mybit, [dst](uint32_t i, uint32_t id) { dst[i] = id; });
             } else {
-                while (nz) {
-                    const uint32_t w = __ffs(nz) - 1u;
-                    nz &= nz - 1u;
-                    const uint32_t word = __shfl_sync(kFull, v, w);
-                    const uint32_t pos = __shfl_sync(kFull, ex, w);
-                    if ((word >> lane) & 1u) {
-                        const uint64_t o = o0 + pos + __popc(word & lt);
-                        if (o < a.capacity) a.ids[o] = my_id + w * 32u;
-                    }
-                }
+                const uint64_t cap = a.capacity;
+                const uint64_t ob = o0;
+                uint32_t* ids = a.ids;
+                expand_unit<false>(v[k], ex, id0, lt, mybit, [=](uint32_t i, uint32_t id) {
+                    if (ob + i < cap) ids[ob + i] = id;
+                });
             }
+            o0 += t;
         }
-        __syncthreads();
     }
     if (lane == 0) bulk_wait_all();
 }
@@ -1081,7 +1086,7 @@ cudaError_t launch_compact_scan(const CompactArgs& a, cudaStream_t s) {
 cudaError_t launch_compact_write(const CompactArgs& a, int sm_count, cudaStream_t s) {
     const uint64_t items = uint64_t(a.n_q) * a.n_chunks;
     if (items == 0) return cudaSuccess;
-    write_ids_kernel<<<grid_for(items, sm_count, 4), 256, 0, s>>>(a);
+    write_ids_kernel<<<grid_for(items, sm_count, 6), 256, 0, s>>>(a);
     count_launch();
     return cudaGetLastError();
 }

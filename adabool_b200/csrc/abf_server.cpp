@@ -606,12 +606,13 @@ abf_status abf_server_destroy(abf_server* s) {
 
 abf_status abf_server_run_trace(abf_server* s, const uint32_t* terms, const uint64_t* offsets, uint32_t n,
                                 const uint64_t* arrival_ns, double timeout_s, uint64_t* h_latency_ns,
-                                uint64_t* h_n_ids, uint8_t* h_paths, abf_trace_stats* out) {
+                                uint64_t* h_queue_ns, uint64_t* h_n_ids, uint8_t* h_paths, abf_trace_stats* out) {
     try {
         if (!s || !offsets || !arrival_ns || !h_latency_ns || (offsets[n] && !terms))
             return fail(ABF_ERR_INVALID, "abf_server_run_trace: bad arguments");
         for (uint32_t i = 0; i < n; ++i) {
             h_latency_ns[i] = ~0ull;
+            if (h_queue_ns) h_queue_ns[i] = ~0ull;
             if (h_n_ids) h_n_ids[i] = 0;
             if (h_paths) h_paths[i] = 0;
             if (i && arrival_ns[i] < arrival_ns[i - 1]) return fail(ABF_ERR_INVALID, "arrivals not ascending");
@@ -649,6 +650,7 @@ abf_status abf_server_run_trace(abf_server* s, const uint32_t* terms, const uint
                 const uint64_t i = r.tag;
                 if (r.status == ABF_OK) {
                     h_latency_ns[i] = r.t_done_ns - r.t_arrival_ns;
+                    if (h_queue_ns) h_queue_ns[i] = r.t_launch_ns - r.t_arrival_ns;
                     if (h_n_ids) h_n_ids[i] = r.n_ids;
                     if (h_paths) h_paths[i] = uint8_t(r.path);
                     ++ts.completed;

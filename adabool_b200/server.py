@@ -100,20 +100,21 @@ class Server:
     def run_trace(self, q_off: np.ndarray, q_terms: np.ndarray, arrival_ns: np.ndarray,
                   timeout_s: float = 120.0) -> dict:
         """Open-loop replay: query i arrives at start + arrival_ns[i]. Returns
-        per-query latency (ns; UINT64_MAX for rejected or failed queries),
-        id counts, paths and the run's totals."""
+        per-query latency and wait before launch (ns; UINT64_MAX for
+        rejected or failed queries), id counts, paths and the run's totals."""
         n = q_off.size - 1
         off = np.ascontiguousarray(q_off, dtype=np.uint64)
         qt = np.ascontiguousarray(q_terms, dtype=np.uint32)
         arr = np.ascontiguousarray(arrival_ns, dtype=np.uint64)
         lat = np.zeros(n, np.uint64)
+        qwait = np.zeros(n, np.uint64)
         nids = np.zeros(n, np.uint64)
         paths = np.zeros(n, np.uint8)
         ts = N.TraceStats()
         N.check(N.lib().abf_server_run_trace(self.handle, N.ptr(qt, N.u32p), N.ptr(off, N.u64p), n,
                                              N.ptr(arr, N.u64p), float(timeout_s), N.ptr(lat, N.u64p),
-                                             N.ptr(nids, N.u64p), N.ptr(paths, N.u8p), C.byref(ts)))
-        return {"latency_ns": lat, "n_ids": nids, "paths": paths, "seconds": ts.seconds,
+                                             N.ptr(qwait, N.u64p), N.ptr(nids, N.u64p), N.ptr(paths, N.u8p), C.byref(ts)))
+        return {"latency_ns": lat, "queue_ns": qwait, "n_ids": nids, "paths": paths, "seconds": ts.seconds,
                 "completed": ts.completed, "rejected": ts.rejected, "failed": ts.failed}
 
     def close(self):

@@ -445,7 +445,8 @@ abf_status abf_server_destroy(abf_server* server);
  * at start + arrival_ns[i] (ascending) by a generator thread, with that
  * time as its arrival; the calling thread polls and releases results as
  * they come. Per query: latency_ns (t_done - arrival; UINT64_MAX when
- * rejected or failed), and optionally n_ids and the path taken. Returns
+ * rejected or failed), and optionally queue_ns (launch - arrival), n_ids
+ * and the path taken. Returns
  * when every query is done, or ABF_ERR_TIMEOUT after timeout_s. */
 typedef struct abf_trace_stats {
     double seconds;              /* first arrival to last completion */
@@ -453,7 +454,8 @@ typedef struct abf_trace_stats {
 } abf_trace_stats;
 abf_status abf_server_run_trace(abf_server* server, const uint32_t* terms, const uint64_t* offsets,
                                 uint32_t n_queries, const uint64_t* arrival_ns, double timeout_s,
-                                uint64_t* h_latency_ns, uint64_t* h_n_ids, uint8_t* h_paths,
+                                uint64_t* h_latency_ns, uint64_t* h_queue_ns, uint64_t* h_n_ids,
+                                uint8_t* h_paths,
                                 abf_trace_stats* out);
 
 /* ------------------------------------------------------------------ */
