@@ -178,8 +178,8 @@ def _train_for_groups(ix, qoff, qt, iso, groups, device, verbose=False):
 
 def serving_experiment(rates=(20_000, 50_000, 100_000, 200_000), offered_seconds: float = 0.5,
                        min_queries: int = 4000, n_train: int = 20_000, label_groups=(32, 256, 1024),
-                       budget_bytes: int = 40 << 30, window_us: int = 200, max_batch_queries: int = 1024,
-                       n_streams: int = 2, device: int = 0, planner_params=None, verbose: bool = False) -> dict:
+                       budget_bytes: int = 40 << 30, window_us: int = 100, max_batch_queries: int = 1024,
+                       n_streams: int = 4, device: int = 0, planner_params=None, verbose: bool = False) -> dict:
     """Config c4: open-loop Poisson arrivals on c1's index, served by the
     batching server with the learned planner, by the same server with the
     fixed threshold rule, and by the plain per-query fixed-rule path (one
@@ -248,6 +248,8 @@ def serving_experiment(rates=(20_000, 50_000, 100_000, 200_000), offered_seconds
                    "rejected": out["rejected"], "failed": out["failed"], "seconds": out["seconds"],
                    "throughput_qps": out["completed"] / max(out["seconds"], 1e-9),
                    **latency_summary(out["latency_ns"]),
+                   "queue_p50_us": float(np.percentile(out["queue_ns"][out["queue_ns"] != np.iinfo(np.uint64).max],
+                                                       50)) / 1e3,
                    "batches": st["batches"], "mean_batch": st["completed"] / max(st["batches"], 1),
                    "max_batch": st["max_batch_queries_seen"], "admission_waits": st["admission_waits"],
                    "peak_reserved_gb": st["peak_reserved_bytes"] / 1e9,
@@ -265,3 +267,56 @@ def serving_experiment(rates=(20_000, 50_000, 100_000, 200_000), offered_seconds
                               "val_mse": tr.val_loss, "seconds": round(train_s, 1)},
             "runs": runs, "tuning": dict(ix.tuning.as_dict(), dense_div=ix.dense_div),
             "seconds": round(time.time() - t_start, 1), "params": tr.params}
+
+
+def index_experiment(configs=("c0", "c1"), path_dir: str = "/tmp", device: int = 0, n_threads: int = 0) -> dict:
+    """On-disk index and builder: per config, the parallel build from COO
+    pairs and from CSR lists (host arrays -> device-resident index), the
+    binary file's size, save time, and load time (one read + uploads)."""
+    import os
+    import torch
+    from . import _native as NN
+    out = {}
+    for c in configs:
+        cfg = W.CONFIGS[c] if isinstance(c, str) else c
+        name = cfg.name
+        L = cfg.lists
+        off, ads = W.gen_lists(L)
+        terms = np.repeat(np.arange(L.n_terms, dtype=np.uint32), np.diff(off).astype(np.int64))
+        rec = {"n_terms": L.n_terms, "n_ads": L.n_ads, "nnz": int(ads.size)}
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ix = Index.from_coo(terms, ads, L.n_terms, L.n_ads, device=device, n_threads=n_threads)
+        torch.cuda.synchronize()
+        rec["build_coo_sorted_s"] = time.perf_counter() - t0
+        del ix
+        perm = np.random.default_rng(7).permutation(terms.size)  # COO pairs in no particular order
+        t_coo, a_coo = terms[perm], ads[perm]
+        del terms, perm
+        t0 = time.perf_counter()
+        ix = Index.from_coo(t_coo, a_coo, L.n_terms, L.n_ads, device=device, n_threads=n_threads)
+        torch.cuda.synchronize()
+        rec["build_coo_shuffled_s"] = time.perf_counter() - t0
+        del ix, t_coo, a_coo
+        t0 = time.perf_counter()
+        ix = Index.from_csr(off, ads, L.n_terms, L.n_ads, device=device, n_threads=n_threads)
+        torch.cuda.synchronize()
+        rec["build_csr_s"] = time.perf_counter() - t0
+        st = ix.stats()
+        rec.update(payload_bytes=st["payload_bytes"], device_bytes=st["device_bytes"])
+        f = os.path.join(path_dir, f"abf_index_{name}.bin")
+        t0 = time.perf_counter()
+        ix.save(f)
+        rec["save_s"] = time.perf_counter() - t0
+        rec["file_bytes"] = os.path.getsize(f)
+        del ix
+        t0 = time.perf_counter()
+        ix2 = Index.load(f, device=device)
+        torch.cuda.synchronize()
+        rec["load_s"] = time.perf_counter() - t0
+        rec["load_gbs"] = rec["file_bytes"] / rec["load_s"] / 1e9
+        del ix2
+        os.remove(f)
+        rec["threads"] = n_threads or os.cpu_count()
+        out[name] = rec
+    return out

@@ -65,9 +65,10 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--out", default="", help="also append the JSON line to this file")
-    p.add_argument("--mode", default="step", choices=["step", "planner", "serve"],
+    p.add_argument("--mode", default="step", choices=["step", "planner", "serve", "index"],
                    help="step: the default benchmark; planner: configs c2/c3 (graph executor, learned planner); "
-                        "serve: config c4 (Poisson arrivals through the serving loop)")
+                        "serve: config c4 (Poisson arrivals through the serving loop); "
+                        "index: parallel builder and binary index file vs the reference's BuildFrom")
     p.add_argument("--rates", default="20000,50000,100000,200000", help="serve mode: arrival rates (queries/s)")
     p.add_argument("--offered-seconds", type=float, default=0.5, help="serve mode: arrivals per rate, in seconds")
     p.add_argument("--planner-out", default="", help="planner mode: save the trained parameters (.npy)")
@@ -509,6 +510,44 @@ def dist_max(x: float, world: int) -> float:
     return x
 
 
+def index_mode() -> dict:
+    """Builder and binary file (ours, c0 / c1 at 1/16 / c1) beside the
+    reference's own BuildFrom (src/AdaBool/inverted_list.h:348-374,
+    compiled from its sources into oracle/_ref) on the same COO pairs, where
+    its single-threaded std::map build finishes in seconds (c0, c1 at 1/16)."""
+    from adabool_b200 import experiments as X
+    from adabool_b200 import workload as W
+    small = [W.CONFIGS["c0"], W.scaled(W.CONFIGS["c1"], 1 / 16)]
+    r = {"metric": "index build / load seconds (host COO or CSR -> device-resident index)",
+         "ours": X.index_experiment(configs=small + [W.CONFIGS["c1"]])}
+    ref = {}
+    try:
+        from oracle import oracle as O
+        if O.ref_build_lib() is None:
+            raise RuntimeError("oracle/_ref/libref_build.so is not built")
+        for cfg in small:
+            name, L = cfg.name, cfg.lists
+            off, ads = W.gen_lists(L)
+            terms = np.repeat(np.arange(L.n_terms, dtype=np.uint32), np.diff(off).astype(np.int64))
+            rec = {"nnz": int(ads.size), "threads": 1,
+                   "note": "reference ivf_list::BuildFrom (host, std::map), no device upload"}
+            t0 = time.perf_counter()
+            m = O.Mixed.from_coo(terms, ads, source="reference")
+            rec["build_from_sorted_s"] = time.perf_counter() - t0
+            m.free()
+            if ads.size <= 10_000_000:  # shuffled pairs: ~2.5 us per pair in its std::map
+                perm = np.random.default_rng(7).permutation(terms.size)
+                t0 = time.perf_counter()
+                m = O.Mixed.from_coo(terms[perm], ads[perm], source="reference")
+                rec["build_from_shuffled_s"] = time.perf_counter() - t0
+                m.free()
+            ref[name] = rec
+    except Exception as e:  # the reference builder is an optional comparison
+        ref["unavailable"] = str(e)
+    r["reference_build_from"] = ref
+    return r
+
+
 def main():
     args = parse()
     if args.mode == "planner" and args.impl == "ours":
@@ -532,6 +571,14 @@ def main():
                                  n_train=min(args.train_queries, 20_000), verbose=True)
         r.pop("params")
         r["metric"] = "serving throughput (queries/s) and p50/p99/p99.9 latency vs per-query fixed-rule path"
+        line = json.dumps(r)
+        print(line, flush=True)
+        if args.out:
+            with open(args.out, "a") as f:
+                f.write(line + "\n")
+        return 0
+    if args.mode == "index" and args.impl == "ours":
+        r = index_mode()
         line = json.dumps(r)
         print(line, flush=True)
         if args.out:
