@@ -448,10 +448,10 @@ abf_status abf_server_default_opts(abf_server_opts* o) {
     if (!o) return fail(ABF_ERR_INVALID, "null opts");
     *o = abf_server_opts{};
     o->budget_bytes = 40ull << 30;
-    o->window_us = 200;
+    o->window_us = 100;
     o->max_batch_queries = 1024;
     o->max_batch_terms = 1ull << 22;
-    o->n_streams = 2;
+    o->n_streams = 4;
     o->path = ABF_PATH_AUTO;
     o->outputs = ABF_SERVE_BITMAPS | ABF_SERVE_IDS;
     return ABF_OK;

@@ -384,10 +384,10 @@ typedef struct abf_server abf_server;
 
 typedef struct abf_server_opts {
     uint64_t budget_bytes;       /* device pool for bitmaps and ids (default 40 GiB) */
-    uint32_t window_us;          /* longest wait of the oldest query before a cut (default 200) */
+    uint32_t window_us;          /* longest wait of the oldest query before a cut (default 100) */
     uint32_t max_batch_queries;  /* default 1024 */
     uint64_t max_batch_terms;    /* default 2^22; also the longest query accepted */
-    uint32_t n_streams;          /* batches in flight, 1..8 (default 2) */
+    uint32_t n_streams;          /* batches in flight, 1..8 (default 4) */
     abf_path path;               /* path of every query; AUTO = installed planner, else fixed rule */
     uint32_t outputs;            /* ABF_SERVE_BITMAPS | ABF_SERVE_IDS (default both) */
 } abf_server_opts;
