@@ -91,11 +91,17 @@ class _Runner:
         return e0.elapsed_time(e1) / reps
 
 
-def autotune(index, q_off: np.ndarray, q_terms: np.ndarray, path: int = N.PATH_HYBRID, sub_batch: int = 64,
-             sample: int = 512, reps: int = 2, rounds: int = 2, knobs: dict | None = None, device: int = 0,
-             verbose: bool = False) -> TuneResult:
-    """Coordinate-descent tuning on the first `sample` queries; leaves the
-    best tuning set on the index and returns it with every trial."""
+GRID = ("dense_div", "heavy_min_len", "tile_words")  # knobs that interact: searched jointly
+
+
+def autotune(index, q_off: np.ndarray, q_terms: np.ndarray, path: int = N.PATH_HYBRID, sub_batch: int = 256,
+             sample: int = 1024, reps: int = 2, rounds: int = 2, knobs: dict | None = None, device: int = 0,
+             grid: bool = True, verbose: bool = False) -> TuneResult:
+    """Tuning on the first `sample` queries: a joint grid over the dense
+    threshold, the merge/scatter switch and the tile width (which lists are
+    dense decides which are merged, and the tile width sets what a merge
+    costs), then coordinate descent over every knob from the grid's best.
+    Leaves the best tuning set on the index and returns it with every trial."""
     n = min(sample, q_off.size - 1)
     run = _Runner(index, q_off[:n + 1], q_terms[:q_off[n]], sub_batch, path, device)
     space = dict(KNOBS if knobs is None else knobs)
@@ -110,6 +116,26 @@ def autotune(index, q_off: np.ndarray, q_terms: np.ndarray, path: int = N.PATH_H
     trials = []
     best_ms = run.time_ms(reps)
     trials.append({"tuning": dict(cur), "ms": best_ms})
+    if grid and all(k in space for k in GRID):
+        best_dd = cur["dense_div"]
+        for dd in space["dense_div"]:
+            index.set_dense_div(dd)
+            for hm in space["heavy_min_len"]:
+                for tw in space["tile_words"]:
+                    cand = dict(cur, dense_div=dd, heavy_min_len=hm, tile_words=tw)
+                    try:
+                        index.set_tuning(heavy_min_len=hm, tile_words=tw)
+                    except N.AbfError:
+                        continue
+                    ms = run.time_ms(1)
+                    trials.append({"tuning": cand, "ms": ms})
+                    if ms < best_ms:
+                        best_ms, cur, best_dd = ms, cand, dd
+        if verbose:
+            print(f"  grid best {best_ms:.3f} ms: {cur}", flush=True)
+        index.set_dense_div(best_dd)
+        apply_cur()
+        best_ms = run.time_ms(reps)
     for _ in range(rounds):
         improved = False
         for knob, values in space.items():
@@ -140,3 +166,21 @@ def autotune(index, q_off: np.ndarray, q_terms: np.ndarray, path: int = N.PATH_H
     if "dense_div" in space:
         index.dense_div = cur["dense_div"]
     return TuneResult(best=dict(cur), best_ms=best_ms, trials=trials)
+
+
+def tune_sub_batch(index, q_off: np.ndarray, q_terms: np.ndarray, path: int = N.PATH_HYBRID,
+                   candidates=(128, 256, 512, 1024), sample: int = 2048, reps: int = 2, device: int = 0) -> dict:
+    """Queries per abf_batch_run call: larger batches let co-resident merge
+    tiles of different queries share L2, smaller ones keep the scatter's
+    working set small. Times each candidate on the same sample."""
+    n = min(sample, q_off.size - 1)
+    out = {}
+    for sb in candidates:
+        if sb > n:
+            continue
+        run = _Runner(index, q_off[:n + 1], q_terms[:q_off[n]], sb, path, device)
+        out[sb] = run.time_ms(reps)
+        run.ws.free()
+        del run
+    best = min(out, key=out.get)
+    return {"best": best, "ms": out}

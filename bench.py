@@ -57,7 +57,8 @@ def parse():
     p.add_argument("--config", default="c1")
     p.add_argument("--scale", type=float, default=1.0, help="shrink the workload (profiling / quick runs)")
     p.add_argument("--queries", type=int, default=0, help="override the query count")
-    p.add_argument("--sub-batch", type=int, default=64)
+    p.add_argument("--sub-batch", type=int, default=0,
+                   help="queries per abf_batch_run call (0: tuned among 128/256/512, 256 without the tuner)")
     p.add_argument("--path", default="hybrid", choices=["auto", "probe", "union", "hybrid", "tile", "planner"])
     p.add_argument("--no-autotune", action="store_true", help="keep the library's default tuning")
     p.add_argument("--tuning", default="", help="apply a saved autotuner result (JSON) instead of tuning")
@@ -194,9 +195,15 @@ def run_ours(args, rank, world, dev):
         # tile, the merge/scatter switch, dense-bitmap threshold, CTAs per SM
         from adabool_b200 import autotune as AT
         t0 = time.time()
-        tr = AT.autotune(ix, qoff, qterms, path=path, sub_batch=args.sub_batch, sample=512, device=dev)
-        tune_info = {"seconds": round(time.time() - t0, 1), "trials": len(tr.trials),
-                     "sample_ms": round(tr.best_ms, 3), "dense_div": tr.best.get("dense_div")}
+        tr = AT.autotune(ix, qoff, qterms, path=path, sub_batch=args.sub_batch or 256, sample=1024, device=dev)
+        tune_info = {"trials": len(tr.trials), "sample_ms": round(tr.best_ms, 3), "dense_div": tr.best.get("dense_div")}
+        if not args.sub_batch:
+            sbt = AT.tune_sub_batch(ix, qoff, qterms, path=path, candidates=(128, 256, 512), device=dev)
+            args.sub_batch = sbt["best"]
+            tune_info["sub_batch_ms"] = {str(k): round(v, 3) for k, v in sbt["ms"].items()}
+        tune_info["seconds"] = round(time.time() - t0, 1)
+    if not args.sub_batch:
+        args.sub_batch = 256
     sbs = split(qoff, qterms, args.sub_batch)
     max_terms = max(int(s[3].size) for s in sbs) + 1
     # id capacity: the bound min(n_ads, sum of list lengths) per query
