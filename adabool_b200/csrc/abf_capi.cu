@@ -140,6 +140,9 @@ struct abf_workspace {
     uint64_t* id_off = nullptr;
     uint8_t* path_out = nullptr;
     uint8_t* auto_paths = nullptr;  // planner choices for ABF_PATH_AUTO batches
+    uint32_t* q_dense = nullptr;    // per term slot: the query's dense bitmaps, packed
+    uint32_t* q_ndense = nullptr;   // per query
+    uint32_t* q_nmerge = nullptr;   // per query
     uint32_t* err = nullptr;
     uint32_t* q_terms = nullptr;  // single-query staging (abf_query)
     uint64_t* q_off = nullptr;
@@ -334,6 +337,9 @@ void ws_release(abf_workspace* w) {
     dev_free(w->id_off);
     dev_free(w->path_out);
     dev_free(w->auto_paths);
+    dev_free(w->q_dense);
+    dev_free(w->q_ndense);
+    dev_free(w->q_nmerge);
     dev_free(w->err);
     dev_free(w->q_terms);
     dev_free(w->q_off);
@@ -357,7 +363,8 @@ abf_status ws_alloc(abf_index* ix, uint32_t max_q, uint64_t max_terms, uint64_t 
         (st = dev_alloc(&w->scan_status, abf::scan_tiles(chunks))) != ABF_OK ||
         (st = dev_alloc(&w->scan_counter, 1)) != ABF_OK || (st = dev_alloc(&w->id_off, uint64_t(max_q) + 1)) != ABF_OK ||
         (st = dev_alloc(&w->path_out, max_q)) != ABF_OK || (st = dev_alloc(&w->err, 1)) != ABF_OK ||
-        (st = dev_alloc(&w->auto_paths, max_q)) != ABF_OK ||
+        (st = dev_alloc(&w->auto_paths, max_q)) != ABF_OK || (st = dev_alloc(&w->q_dense, max_terms)) != ABF_OK ||
+        (st = dev_alloc(&w->q_ndense, max_q)) != ABF_OK || (st = dev_alloc(&w->q_nmerge, max_q)) != ABF_OK ||
         (st = dev_alloc(&w->q_terms, max_terms)) != ABF_OK || (st = dev_alloc(&w->q_off, 2)) != ABF_OK) {
         ws_release(w);
         return st;
@@ -436,6 +443,9 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
     pa.err = ws->err;
     pa.dense_in_tile = 1;
     pa.tile_cls = ws->tile_cls;
+    pa.q_dense = ws->q_dense;
+    pa.q_ndense = ws->q_ndense;
+    pa.q_nmerge = ws->q_nmerge;
     if (!b->d_paths && b->path == ABF_PATH_AUTO && ix->dev.planner) {
         // learned planner: per-query path from the fused feature + MLP kernel
         TIMED(K_PLANNER, abf::launch_planner(v, ix->dev.planner, b->d_terms, b->d_offsets, b->n_queries,
@@ -463,6 +473,9 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
     ta.n_words = n_words;
     ta.accumulate = 0;
     ta.vec_ok = (reinterpret_cast<uintptr_t>(b->d_bitmaps) % 16 == 0) && (b->bitmap_stride_words % 4 == 0);
+    ta.q_dense = ws->q_dense;
+    ta.q_ndense = ws->q_ndense;
+    ta.q_nmerge = ws->q_nmerge;
     TIMED(K_TILE, abf::launch_tile_union(v, ta, t, ix->sm_count, s));
     abf::ScatterArgs sa{};
     sa.terms = b->d_terms;

@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(256) plan_kernel(IndexView ix, PlanArgs a) {
         const uint32_t hm = path == ABF_PATH_TILE ? 0u
                             : path == ABF_PATH_HYBRID ? a.hybrid_min
                             : probe ? kNoHeavy : kDenseOnly;
-        uint32_t carry = 0;
+        uint32_t carry = 0, dcarry = 0, mcarry = 0;
         for (uint64_t c0 = qb; c0 < qe; c0 += 256) {
             const uint64_t i = c0 + tid;
             uint32_t cnt = 0, cls = kNone;
@@ -294,11 +294,26 @@ __global__ void __launch_bounds__(256) plan_kernel(IndexView ix, PlanArgs a) {
             const uint32_t ex = block_excl_scan<256>(cnt, s_warp, &tot);
             if (i < qe) a.term_lpref[i] = carry + ex;
             carry += tot;
+            if (a.q_dense) {
+                // dense bitmaps packed in term order (low half) and merged
+                // lists without one (high half), counted in one scan
+                const bool dn = cls != kNone && (cls & kDenseFlag);
+                const uint32_t flags = (dn ? 1u : 0u) | ((cls != kNone && !dn) ? 0x10000u : 0u);
+                uint32_t ftot;
+                const uint32_t fex = block_excl_scan<256>(flags, s_warp, &ftot);
+                if (dn) a.q_dense[qb + dcarry + (fex & 0xffffu)] = cls & ~kDenseFlag;
+                dcarry += ftot & 0xffffu;
+                mcarry += ftot >> 16;
+            }
         }
         if (tid == 0) {
             a.heavy_min[q] = probe ? kNoHeavy : hm;
             a.q_light_cnt[q] = carry;
             if (a.path_out) a.path_out[q] = uint8_t(path);
+            if (a.q_dense) {
+                a.q_ndense[q] = dcarry;
+                a.q_nmerge[q] = mcarry;
+            }
         }
         __syncthreads();
     }
@@ -385,6 +400,51 @@ __device__ __forceinline__ uint32_t find_slot(const uint32_t* s_pref, uint32_t f
     return a0;
 }
 
+// One tile of a query whose merged lists all have dense bitmaps: the OR of
+// the nd slices [t*W, t*W + nw) of the bitmaps listed in dl, written to dst.
+template <int W, int NT>
+__device__ __forceinline__ void dense_only_tile(const IndexView& ix, const uint32_t* dl, uint32_t nd, uint32_t t,
+                                                uint32_t* dst, uint32_t nw, bool vec_ok) {
+    constexpr uint32_t KT = 8;
+    const uint32_t tid = threadIdx.x;
+    const uint64_t tw = uint64_t(t) * W;
+    if (vec_ok) {
+        const uint4* base = reinterpret_cast<const uint4*>(ix.dense + tw);
+        const uint64_t st4 = ix.dense_stride / 4;
+        uint4* d4 = reinterpret_cast<uint4*>(dst);
+        const uint32_t n4 = nw / 4u;
+        for (uint32_t j = tid; j < n4; j += NT) {
+            uint4 acc = make_uint4(0u, 0u, 0u, 0u);
+            uint32_t k = 0;
+            for (; k + KT <= nd; k += KT) {
+                uint4 x[KT];
+#pragma unroll
+                for (uint32_t e = 0; e < KT; ++e) x[e] = __ldg(base + uint64_t(__ldg(dl + k + e)) * st4 + j);
+#pragma unroll
+                for (uint32_t e = 0; e < KT; ++e) {
+                    acc.x |= x[e].x; acc.y |= x[e].y; acc.z |= x[e].z; acc.w |= x[e].w;
+                }
+            }
+            for (; k < nd; ++k) {
+                const uint4 x = __ldg(base + uint64_t(__ldg(dl + k)) * st4 + j);
+                acc.x |= x.x; acc.y |= x.y; acc.z |= x.z; acc.w |= x.w;
+            }
+            d4[j] = acc;
+        }
+        for (uint32_t i = n4 * 4u + tid; i < nw; i += NT) {
+            uint32_t acc = 0;
+            for (uint32_t k = 0; k < nd; ++k) acc |= __ldg(ix.dense + uint64_t(__ldg(dl + k)) * ix.dense_stride + tw + i);
+            dst[i] = acc;
+        }
+    } else {
+        for (uint32_t i = tid; i < nw; i += NT) {
+            uint32_t acc = 0;
+            for (uint32_t k = 0; k < nd; ++k) acc |= __ldg(ix.dense + uint64_t(__ldg(dl + k)) * ix.dense_stride + tw + i);
+            dst[i] = acc;
+        }
+    }
+}
+
 template <int W, int NW>
 __global__ void __launch_bounds__(NW * 32) tile_union_kernel(IndexView ix, TileArgs a) {
     constexpr int NT = NW * 32;
@@ -418,6 +478,13 @@ __global__ void __launch_bounds__(NW * 32) tile_union_kernel(IndexView ix, TileA
         if (hm == kNoHeavy || qb == qe) {  // nothing to merge: leave or zero the tile
             if (!a.accumulate)
                 for (uint32_t i = tid; i < nw; i += NT) dst[i] = 0u;
+            continue;
+        }
+        if (a.q_dense && !a.accumulate && a.q_nmerge[q] == 0) {
+            // every merged list has a dense bitmap: each thread ORs its
+            // 16-byte slots over the query's dense slices, KT loads in
+            // flight, and stores the result; no shared tile, no barrier
+            dense_only_tile<W, NT>(ix, a.q_dense + qb, a.q_ndense[q], t, dst, nw, a.vec_ok != 0);
             continue;
         }
         for (uint32_t i = tid; i < uint32_t(W); i += NT) tile[i] = (a.accumulate && i < nw) ? dst[i] : 0u;

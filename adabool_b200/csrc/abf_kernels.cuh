@@ -57,6 +57,10 @@ struct PlanArgs {
     int dense_in_tile;        // 1: dense-bitmap lists go to the merge kernel, 0: scattered too
     uint32_t* tile_cls;       // out: per term slot, what the merge kernel does with it
                               // (kNone: nothing, kDenseFlag | d: dense bitmap d, else the term)
+    uint32_t* q_dense;        // out (optional): per query, its dense bitmap indices packed
+                              // from the query's first term slot on
+    uint32_t* q_ndense;       // out (with q_dense): per query, dense bitmaps to merge
+    uint32_t* q_nmerge;       // out (with q_dense): per query, merged lists without a dense bitmap
 };
 
 constexpr uint32_t kDenseFlag = 0x80000000u;
@@ -89,6 +93,9 @@ struct TileArgs {
     uint64_t n_words;         // words of one bitmap
     int accumulate;           // 1: OR into the existing bitmap, 0: overwrite
     int vec_ok;               // out 16-byte aligned and out_stride % 4 == 0
+    const uint32_t* q_dense;  // optional (plan kernel): queries whose merged lists all have
+    const uint32_t* q_ndense; // dense bitmaps take a barrier-free path that streams the OR of
+    const uint32_t* q_nmerge; // their slices straight to the output
 };
 
 struct ScatterArgs {
