@@ -29,6 +29,7 @@ KNOBS = {
     "ctas_per_sm": [2, 4, 6, 8],
     "scatter_blocks_per_warp": [1, 2, 4, 8],
     "dense_div": [16, 32, 64, 128, 256],  # lists with len * dense_div >= n_ads get dense bitmaps
+    "group_min_queries": [0, 32],  # 0: no dense group kernel
 }
 
 
@@ -91,7 +92,10 @@ class _Runner:
         return e0.elapsed_time(e1) / reps
 
 
-GRID = ("dense_div", "heavy_min_len", "tile_words")  # knobs that interact: searched jointly
+# knobs that interact, searched jointly: which lists are dense decides which
+# are merged, the tile width sets what a merge costs, and the group kernel
+# changes what a dense list costs
+GRID = ("dense_div", "heavy_min_len", "tile_words", "group_min_queries")
 
 
 def autotune(index, q_off: np.ndarray, q_terms: np.ndarray, path: int = N.PATH_HYBRID, sub_batch: int = 256,
@@ -117,20 +121,22 @@ def autotune(index, q_off: np.ndarray, q_terms: np.ndarray, path: int = N.PATH_H
     best_ms = run.time_ms(reps)
     trials.append({"tuning": dict(cur), "ms": best_ms})
     if grid and all(k in space for k in GRID):
+        import itertools
         best_dd = cur["dense_div"]
+        rest = GRID[1:]
         for dd in space["dense_div"]:
             index.set_dense_div(dd)
-            for hm in space["heavy_min_len"]:
-                for tw in space["tile_words"]:
-                    cand = dict(cur, dense_div=dd, heavy_min_len=hm, tile_words=tw)
-                    try:
-                        index.set_tuning(heavy_min_len=hm, tile_words=tw)
-                    except N.AbfError:
-                        continue
-                    ms = run.time_ms(1)
-                    trials.append({"tuning": cand, "ms": ms})
-                    if ms < best_ms:
-                        best_ms, cur, best_dd = ms, cand, dd
+            for vals in itertools.product(*(space[k] for k in rest)):
+                kv = dict(zip(rest, vals))
+                cand = dict(cur, dense_div=dd, **kv)
+                try:
+                    index.set_tuning(**kv)
+                except N.AbfError:
+                    continue
+                ms = run.time_ms(1)
+                trials.append({"tuning": cand, "ms": ms})
+                if ms < best_ms:
+                    best_ms, cur, best_dd = ms, cand, dd
         if verbose:
             print(f"  grid best {best_ms:.3f} ms: {cur}", flush=True)
         index.set_dense_div(best_dd)

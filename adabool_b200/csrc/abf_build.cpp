@@ -288,7 +288,8 @@ void derive_tables(const HostIndex& h, uint32_t dense_div, int n_threads, Derive
     const uint64_t budget = std::max<uint64_t>(256ull << 20, 2ull * 16ull * h.payload.size());
     std::vector<uint32_t> dense_terms;
     for (uint32_t t : cand) {
-        if ((dense_terms.size() + 1) * out->dense_stride * 4 > budget) break;
+        // 16-bit bitmap indices in the merge kernels' per-query lists
+        if ((dense_terms.size() + 1) * out->dense_stride * 4 > budget || dense_terms.size() >= 65535) break;
         out->term_dense[t] = uint32_t(dense_terms.size());
         dense_terms.push_back(t);
     }

@@ -57,10 +57,10 @@ namespace {
 
 // ---- kernel timing (abf_profile_enable / abf_profile_read) ----
 enum Kid { K_PLAN, K_QUEUE, K_PROBE_BITS, K_TILE, K_SCATTER, K_PROBE, K_COUNT, K_SCAN, K_WRITE, K_PLANNER,
-           K_NKERNELS };
+           K_GROUP, K_NKERNELS };
 const char* const kKernelNames[K_NKERNELS] = {"plan",   "queue_scan",    "probe_bits",   "tile_union",
                                               "scatter_union", "probe", "compact_count", "compact_scan",
-                                              "compact_write", "planner"};
+                                              "compact_write", "planner",    "dense_group"};
 
 struct Profiler {
     struct Rec {
@@ -140,9 +140,10 @@ struct abf_workspace {
     uint64_t* id_off = nullptr;
     uint8_t* path_out = nullptr;
     uint8_t* auto_paths = nullptr;  // planner choices for ABF_PATH_AUTO batches
-    uint32_t* q_dense = nullptr;    // per term slot: the query's dense bitmaps, packed
+    uint16_t* q_dense16 = nullptr;  // the queries' dense bitmap lists (see PlanArgs)
+    uint32_t* q_dstart = nullptr;   // per query
     uint32_t* q_ndense = nullptr;   // per query
-    uint32_t* q_nmerge = nullptr;   // per query
+    uint32_t* q_dmode = nullptr;    // per query
     uint32_t* err = nullptr;
     uint32_t* q_terms = nullptr;  // single-query staging (abf_query)
     uint64_t* q_off = nullptr;
@@ -222,6 +223,7 @@ void default_tuning(abf_index* ix) {
     t.ctas_per_sm = 6;
     t.probe_cap = 32;
     t.probe_min_fraction = 0.5f;
+    t.group_min_queries = 32;
 }
 
 void free_device(abf_index* ix) {
@@ -337,9 +339,10 @@ void ws_release(abf_workspace* w) {
     dev_free(w->id_off);
     dev_free(w->path_out);
     dev_free(w->auto_paths);
-    dev_free(w->q_dense);
+    dev_free(w->q_dense16);
+    dev_free(w->q_dstart);
     dev_free(w->q_ndense);
-    dev_free(w->q_nmerge);
+    dev_free(w->q_dmode);
     dev_free(w->err);
     dev_free(w->q_terms);
     dev_free(w->q_off);
@@ -363,8 +366,10 @@ abf_status ws_alloc(abf_index* ix, uint32_t max_q, uint64_t max_terms, uint64_t 
         (st = dev_alloc(&w->scan_status, abf::scan_tiles(chunks))) != ABF_OK ||
         (st = dev_alloc(&w->scan_counter, 1)) != ABF_OK || (st = dev_alloc(&w->id_off, uint64_t(max_q) + 1)) != ABF_OK ||
         (st = dev_alloc(&w->path_out, max_q)) != ABF_OK || (st = dev_alloc(&w->err, 1)) != ABF_OK ||
-        (st = dev_alloc(&w->auto_paths, max_q)) != ABF_OK || (st = dev_alloc(&w->q_dense, max_terms)) != ABF_OK ||
-        (st = dev_alloc(&w->q_ndense, max_q)) != ABF_OK || (st = dev_alloc(&w->q_nmerge, max_q)) != ABF_OK ||
+        (st = dev_alloc(&w->auto_paths, max_q)) != ABF_OK ||
+        (st = dev_alloc(&w->q_dense16, max_terms + 8ull * max_q + 16)) != ABF_OK ||
+        (st = dev_alloc(&w->q_dstart, max_q)) != ABF_OK || (st = dev_alloc(&w->q_ndense, max_q)) != ABF_OK ||
+        (st = dev_alloc(&w->q_dmode, max_q)) != ABF_OK ||
         (st = dev_alloc(&w->q_terms, max_terms)) != ABF_OK || (st = dev_alloc(&w->q_off, 2)) != ABF_OK) {
         ws_release(w);
         return st;
@@ -443,9 +448,10 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
     pa.err = ws->err;
     pa.dense_in_tile = 1;
     pa.tile_cls = ws->tile_cls;
-    pa.q_dense = ws->q_dense;
+    pa.q_dense16 = ws->q_dense16;
+    pa.q_dstart = ws->q_dstart;
     pa.q_ndense = ws->q_ndense;
-    pa.q_nmerge = ws->q_nmerge;
+    pa.q_dmode = ws->q_dmode;
     if (!b->d_paths && b->path == ABF_PATH_AUTO && ix->dev.planner) {
         // learned planner: per-query path from the fused feature + MLP kernel
         TIMED(K_PLANNER, abf::launch_planner(v, ix->dev.planner, b->d_terms, b->d_offsets, b->n_queries,
@@ -473,9 +479,42 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
     ta.n_words = n_words;
     ta.accumulate = 0;
     ta.vec_ok = (reinterpret_cast<uintptr_t>(b->d_bitmaps) % 16 == 0) && (b->bitmap_stride_words % 4 == 0);
-    ta.q_dense = ws->q_dense;
+    ta.q_dense16 = ws->q_dense16;
+    ta.q_dstart = ws->q_dstart;
     ta.q_ndense = ws->q_ndense;
-    ta.q_nmerge = ws->q_nmerge;
+    ta.q_dmode = ws->q_dmode;
+    // dense group kernel: every dense-only query's tiles in one pass per
+    // 32-word tile, when the batch is large enough and the dense bitmaps
+    // (plus the zero row) fit three TMA boxes of 256
+    const uint32_t n_dense = v.n_dense;
+    bool group = t.group_min_queries && b->n_queries >= t.group_min_queries &&
+                 b->n_queries <= abf::kGroupMaxQueries && n_dense > 0 &&
+                 n_dense + 1 <= abf::kGroupMaxBoxes * abf::kGroupBoxRows;
+    if (group && (ix->dense_tmap_base != ix->dev.dense || ix->dense_tmap_rows != n_dense)) {
+        if (abf::encode_dense_tmap(v, ix->dense_tmap) == cudaSuccess) {
+            ix->dense_tmap_base = ix->dev.dense;
+            ix->dense_tmap_rows = n_dense;
+        } else {
+            group = false;
+        }
+    }
+    ta.skip_dense_only = group ? 1 : 0;
+    if (group) {
+        abf::DenseGroupArgs ga{};
+        ga.q_dense16 = ws->q_dense16;
+        ga.q_dstart = ws->q_dstart;
+        ga.q_ndense = ws->q_ndense;
+        ga.q_dmode = ws->q_dmode;
+        ga.n_q = b->n_queries;
+        ga.n_rows = n_dense + 1;
+        ga.list_cap = abf::dense_group_list_cap(ga.n_rows, b->n_queries);
+        ga.n_tiles = uint32_t((n_words + abf::kGroupTileWords - 1) / abf::kGroupTileWords);
+        ga.out = b->d_bitmaps;
+        ga.out_stride = b->bitmap_stride_words;
+        ga.n_words = n_words;
+        ga.err = ws->err;
+        TIMED(K_GROUP, abf::launch_dense_group(ix->dense_tmap, ga, ix->sm_count, s));
+    }
     TIMED(K_TILE, abf::launch_tile_union(v, ta, t, ix->sm_count, s));
     abf::ScatterArgs sa{};
     sa.terms = b->d_terms;

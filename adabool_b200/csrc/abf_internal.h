@@ -124,6 +124,7 @@ struct IndexView {
     const uint32_t* dir;
     const uint32_t* term_cbytes;
     uint64_t dense_stride;
+    uint32_t n_dense;
     uint32_t dir_n;
     uint32_t n_terms;
     uint32_t n_ads;
@@ -159,6 +160,11 @@ struct abf_index {
     void* h_stage = nullptr;          // pinned staging for abf_query terms
     size_t h_stage_bytes = 0;
     void* stage_event = nullptr;      // cudaEvent_t guarding the staging buffer
+    // TMA descriptor of the dense bitmaps (2-D: words x bitmaps), encoded on
+    // first use and again when the dense bitmaps change
+    alignas(64) unsigned char dense_tmap[256] = {};
+    const void* dense_tmap_base = nullptr;
+    uint32_t dense_tmap_rows = 0;
 };
 
 namespace abf {

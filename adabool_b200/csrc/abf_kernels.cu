@@ -14,6 +14,9 @@
 //       (test/adsfilter_batch.cu:82-97)
 #include "abf_kernels.cuh"
 
+#include <cuda.h>
+#include <cstring>
+
 #include <algorithm>
 #include <atomic>
 
@@ -239,6 +242,7 @@ __global__ void __launch_bounds__(256) plan_kernel(IndexView ix, PlanArgs a) {
     __shared__ uint32_t s_warp[32];
     __shared__ unsigned long long s_red[8];
     __shared__ uint32_t s_path;
+    __shared__ uint32_t s_mask[2048];  // the query's dense bitmaps (n_dense <= 65535)
     const uint32_t tid = threadIdx.x;
     for (uint32_t q = blockIdx.x; q < a.n_q; q += gridDim.x) {
         uint64_t qb = a.q_off[q], qe = a.q_off[q + 1];
@@ -275,7 +279,13 @@ __global__ void __launch_bounds__(256) plan_kernel(IndexView ix, PlanArgs a) {
         const uint32_t hm = path == ABF_PATH_TILE ? 0u
                             : path == ABF_PATH_HYBRID ? a.hybrid_min
                             : probe ? kNoHeavy : kDenseOnly;
-        uint32_t carry = 0, dcarry = 0, mcarry = 0;
+        const bool want_d = a.q_dense16 != nullptr;
+        const uint32_t mw = (ix.n_dense + 31u) / 32u;
+        if (want_d) {
+            for (uint32_t i = tid; i < mw; i += 256) s_mask[i] = 0u;
+            __syncthreads();
+        }
+        uint32_t carry = 0, nmerge = 0;
         for (uint64_t c0 = qb; c0 < qe; c0 += 256) {
             const uint64_t i = c0 + tid;
             uint32_t cnt = 0, cls = kNone;
@@ -294,26 +304,46 @@ __global__ void __launch_bounds__(256) plan_kernel(IndexView ix, PlanArgs a) {
             const uint32_t ex = block_excl_scan<256>(cnt, s_warp, &tot);
             if (i < qe) a.term_lpref[i] = carry + ex;
             carry += tot;
-            if (a.q_dense) {
-                // dense bitmaps packed in term order (low half) and merged
-                // lists without one (high half), counted in one scan
-                const bool dn = cls != kNone && (cls & kDenseFlag);
-                const uint32_t flags = (dn ? 1u : 0u) | ((cls != kNone && !dn) ? 0x10000u : 0u);
-                uint32_t ftot;
-                const uint32_t fex = block_excl_scan<256>(flags, s_warp, &ftot);
-                if (dn) a.q_dense[qb + dcarry + (fex & 0xffffu)] = cls & ~kDenseFlag;
-                dcarry += ftot & 0xffffu;
-                mcarry += ftot >> 16;
+            if (want_d && cls != kNone) {
+                if (cls & kDenseFlag) {
+                    const uint32_t d = cls & ~kDenseFlag;
+                    atomicOr(&s_mask[d >> 5], 1u << (d & 31u));
+                } else {
+                    ++nmerge;
+                }
+            }
+        }
+        if (want_d) {
+            // the query's distinct dense bitmaps in ascending order: each
+            // thread expands a contiguous run of mask words at its prefix
+            const uint32_t any_merge = __syncthreads_or(nmerge);
+            const uint32_t per = (mw + 255u) / 256u;
+            const uint32_t w0 = tid * per < mw ? tid * per : mw;
+            const uint32_t w1 = w0 + per < mw ? w0 + per : mw;
+            uint32_t c = 0;
+            for (uint32_t w = w0; w < w1; ++w) c += __popc(s_mask[w]);
+            uint32_t nd;
+            uint32_t o = block_excl_scan<256>(c, s_warp, &nd);
+            const uint32_t start = uint32_t((qb + 8ull * q + 7ull) & ~7ull);
+            uint16_t* dst = a.q_dense16 + start;
+            for (uint32_t w = w0; w < w1; ++w) {
+                uint32_t m = s_mask[w];
+                while (m) {
+                    dst[o++] = uint16_t(w * 32u + uint32_t(__ffs(m)) - 1u);
+                    m &= m - 1u;
+                }
+            }
+            for (uint32_t i = nd + tid; i < ((nd + 7u) & ~7u); i += 256) dst[i] = uint16_t(ix.n_dense);
+            if (tid == 0) {
+                a.q_dstart[q] = start;
+                a.q_ndense[q] = nd;
+                a.q_dmode[q] = (!probe && qe > qb && !any_merge) ? 1u : 0u;
             }
         }
         if (tid == 0) {
             a.heavy_min[q] = probe ? kNoHeavy : hm;
             a.q_light_cnt[q] = carry;
             if (a.path_out) a.path_out[q] = uint8_t(path);
-            if (a.q_dense) {
-                a.q_ndense[q] = dcarry;
-                a.q_nmerge[q] = mcarry;
-            }
         }
         __syncthreads();
     }
@@ -403,7 +433,7 @@ __device__ __forceinline__ uint32_t find_slot(const uint32_t* s_pref, uint32_t f
 // One tile of a query whose merged lists all have dense bitmaps: the OR of
 // the nd slices [t*W, t*W + nw) of the bitmaps listed in dl, written to dst.
 template <int W, int NT>
-__device__ __forceinline__ void dense_only_tile(const IndexView& ix, const uint32_t* dl, uint32_t nd, uint32_t t,
+__device__ __forceinline__ void dense_only_tile(const IndexView& ix, const uint16_t* dl, uint32_t nd, uint32_t t,
                                                 uint32_t* dst, uint32_t nw, bool vec_ok) {
     constexpr uint32_t KT = 8;
     const uint32_t tid = threadIdx.x;
@@ -480,11 +510,13 @@ __global__ void __launch_bounds__(NW * 32) tile_union_kernel(IndexView ix, TileA
                 for (uint32_t i = tid; i < nw; i += NT) dst[i] = 0u;
             continue;
         }
-        if (a.q_dense && !a.accumulate && a.q_nmerge[q] == 0) {
-            // every merged list has a dense bitmap: each thread ORs its
-            // 16-byte slots over the query's dense slices, KT loads in
-            // flight, and stores the result; no shared tile, no barrier
-            dense_only_tile<W, NT>(ix, a.q_dense + qb, a.q_ndense[q], t, dst, nw, a.vec_ok != 0);
+        if (a.q_dense16 && !a.accumulate && a.q_dmode[q]) {
+            // every merged list has a dense bitmap: the dense group kernel
+            // writes this tile, or each thread ORs its 16-byte slots over the
+            // query's dense slices, KT loads in flight, and stores the
+            // result; no shared tile, no barrier
+            if (!a.skip_dense_only)
+                dense_only_tile<W, NT>(ix, a.q_dense16 + a.q_dstart[q], a.q_ndense[q], t, dst, nw, a.vec_ok != 0);
             continue;
         }
         for (uint32_t i = tid; i < uint32_t(W); i += NT) tile[i] = (a.accumulate && i < nw) ? dst[i] : 0u;
@@ -587,6 +619,166 @@ __global__ void __launch_bounds__(NW * 32) tile_union_kernel(IndexView ix, TileA
             for (uint32_t i = tid; i < nw; i += NT) dst[i] = tile[i];
         }
         __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// list-union, dense group variant: one CTA per SM walks 32-word tiles; for
+// each tile, a 2-D TMA copy stages that tile's slice of every dense bitmap
+// in shared memory once (double-buffered: the next tile's copy is in flight
+// while this one is merged), then every dense-only query of the batch ORs
+// its dense slices from shared memory and writes its 32 words. Dense bitmaps
+// shared by many queries are read from L2 / HBM once per tile instead of
+// once per query and tile.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
+        : "memory");
+}
+
+constexpr uint32_t kGroupThreads = 1024;
+
+// OR of the 8 rows named by the 16-bit indices in v, column `lane`
+__device__ __forceinline__ uint32_t or8(const uint32_t* S, uint4 v, uint32_t lane) {
+    return S[(v.x & 0xffffu) * kGroupTileWords + lane] | S[(v.x >> 16) * kGroupTileWords + lane] |
+           S[(v.y & 0xffffu) * kGroupTileWords + lane] | S[(v.y >> 16) * kGroupTileWords + lane] |
+           S[(v.z & 0xffffu) * kGroupTileWords + lane] | S[(v.z >> 16) * kGroupTileWords + lane] |
+           S[(v.w & 0xffffu) * kGroupTileWords + lane] | S[(v.w >> 16) * kGroupTileWords + lane];
+}
+
+// OR over a query's list of nd row indices (padded to a multiple of 8 with
+// the zero row), read 16 at a time from shared or global memory
+__device__ __forceinline__ uint32_t or_list(const uint32_t* S, const uint4* dl, uint32_t nd, uint32_t lane) {
+    uint32_t acc = 0, k = 0;
+    for (; k + 16u <= nd; k += 16u) {
+        const uint4 v0 = dl[k >> 3], v1 = dl[(k >> 3) + 1];
+        acc |= or8(S, v0, lane) | or8(S, v1, lane);
+    }
+    if (k < nd) acc |= or8(S, dl[k >> 3], lane);
+    if (k + 8u < nd) acc |= or8(S, dl[(k >> 3) + 1], lane);
+    return acc;
+}
+
+// Shared memory (dynamic, 1024-byte aligned base): two stages of n_rows x
+// 32 words (rows = dense bitmaps + the zero row), then per dense-only query
+// its list's offset and length, the queue of dense-only queries, and the
+// lists themselves when they fit (else they are read from global memory).
+__global__ void __launch_bounds__(kGroupThreads, 1)
+    dense_group_kernel(const __grid_constant__ CUtensorMap tmap_full, const __grid_constant__ CUtensorMap tmap_last,
+                       DenseGroupArgs a) {
+    extern __shared__ uint8_t g_raw[];
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ uint32_t s_next[2];
+    __shared__ uint32_t s_fail, s_ndq;
+    __shared__ uint32_t s_warp[32];
+    uint8_t* base = g_raw + ((1024u - (smem_addr(g_raw) & 1023u)) & 1023u);
+    const uint32_t stage_bytes = (a.n_rows * kGroupTileWords * 4u + 1023u) & ~1023u;
+    uint32_t* stage0 = reinterpret_cast<uint32_t*>(base);
+    uint32_t* s_meta = reinterpret_cast<uint32_t*>(base + 2u * stage_bytes);  // n_q: list offset / 8 << 16 | nd
+    uint16_t* s_qlist = reinterpret_cast<uint16_t*>(s_meta + a.n_q);          // dense-only queries
+    uint4* s_lists = reinterpret_cast<uint4*>(base + 2u * stage_bytes + ((6u * a.n_q + 15u) & ~15u));
+    const uint32_t tid = threadIdx.x, lane = lane_id(), warp = warp_id();
+    constexpr uint32_t kNW = kGroupThreads / 32u;
+    uint32_t t = blockIdx.x;
+    if (t >= a.n_tiles) return;
+    const uint32_t full_boxes = (a.n_rows - 1u) / kGroupBoxRows;  // boxes of 256 rows before the last
+    auto issue = [&](uint32_t tile, uint32_t st) {  // thread 0 only
+        fence_proxy_async();  // earlier reads of this stage (ordered by the barrier) before the copy
+        mbar_expect_tx(&bar[st], a.n_rows * kGroupTileWords * 4u);
+        uint32_t* dst = stage0 + st * (stage_bytes / 4u);
+        for (uint32_t j = 0; j < full_boxes; ++j)
+            tma_load_2d(dst + j * kGroupBoxRows * kGroupTileWords, &tmap_full, int(tile * kGroupTileWords),
+                        int(j * kGroupBoxRows), &bar[st]);
+        tma_load_2d(dst + full_boxes * kGroupBoxRows * kGroupTileWords, &tmap_last, int(tile * kGroupTileWords),
+                    int(full_boxes * kGroupBoxRows), &bar[st]);
+    };
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+        s_next[0] = s_next[1] = 0;
+        s_fail = 0;
+        issue(t, 0);  // the first tile's copy overlaps the list staging below
+    }
+    // stage the dense-only queries' lists (the same for every tile): offsets
+    // by a block scan over the queries, at most two per thread
+    uint32_t len[2], cnt[2];
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        const uint32_t q = tid * 2u + r;
+        const bool dq = q < a.n_q && a.q_dmode[q];
+        len[r] = dq ? ((a.q_ndense[q] + 7u) & ~7u) : 0u;
+        cnt[r] = dq ? 1u : 0u;
+    }
+    uint32_t tot_len, tot_cnt;
+    const uint32_t off0 = block_excl_scan<kGroupThreads>(len[0] + len[1], s_warp, &tot_len);
+    const uint32_t rk0 = block_excl_scan<kGroupThreads>(cnt[0] + cnt[1], s_warp, &tot_cnt);
+    const bool in_smem = tot_len <= a.list_cap;
+    {
+        uint32_t off = off0, rk = rk0;
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const uint32_t q = tid * 2u + r;
+            if (q < a.n_q) s_meta[q] = cnt[r] ? ((off >> 3) << 16) | a.q_ndense[q] : 0xffffffffu;
+            if (cnt[r]) s_qlist[rk] = uint16_t(q);
+            off += len[r];
+            rk += cnt[r];
+        }
+    }
+    if (tid == 0) s_ndq = tot_cnt;
+    __syncthreads();
+    if (in_smem) {
+        for (uint32_t i = warp; i < tot_cnt; i += kNW) {  // a warp per query, 16 bytes per lane
+            const uint32_t q = s_qlist[i];
+            const uint32_t m = s_meta[q];
+            const uint4* src = reinterpret_cast<const uint4*>(a.q_dense16 + a.q_dstart[q]);
+            for (uint32_t j = lane; j < ((m & 0xffffu) + 7u) / 8u; j += 32u) s_lists[(m >> 16) + j] = src[j];
+        }
+    }
+    __syncthreads();
+    const uint32_t n_dq = s_ndq;
+    uint32_t phase = 0;  // bit s: parity of stage s's next completion
+    for (uint32_t it = 0; t < a.n_tiles; ++it, t += gridDim.x) {
+        const uint32_t st = it & 1u;
+        const bool more = t + gridDim.x < a.n_tiles;
+        if (tid == 0 && more) issue(t + gridDim.x, st ^ 1u);
+        uint32_t spins = 0;
+        while (!mbar_try_wait(&bar[st], (phase >> st) & 1u)) {
+            if (++spins > kSpinLimit) {
+                s_fail = 1;
+                break;
+            }
+        }
+        phase ^= 1u << st;
+        if (__syncthreads_or(s_fail)) {
+            if (tid == 0) atomicOr(a.err, kErrTmaTimeout);
+            if (more) {  // let the other stage's copy land before the CTA leaves
+                uint32_t sp = 0;
+                while (!mbar_try_wait(&bar[st ^ 1u], (phase >> (st ^ 1u)) & 1u) && ++sp < kSpinLimit) {
+                }
+            }
+            return;
+        }
+        const uint32_t* S = stage0 + st * (stage_bytes / 4u);
+        const uint64_t w = uint64_t(t) * kGroupTileWords + lane;
+        for (;;) {
+            uint32_t i = 0;
+            if (lane == 0) i = atomicAdd(&s_next[st], 1u);
+            i = __shfl_sync(kFull, i, 0);
+            if (i >= n_dq) break;
+            const uint32_t q = s_qlist[i];
+            const uint32_t m = s_meta[q];
+            const uint32_t nd = m & 0xffffu;
+            const uint32_t acc =
+                in_smem ? or_list(S, s_lists + (m >> 16), nd, lane)
+                        : or_list(S, reinterpret_cast<const uint4*>(a.q_dense16 + a.q_dstart[q]), nd, lane);
+            if (w < a.n_words) a.out[uint64_t(q) * a.out_stride + w] = acc;
+        }
+        __syncthreads();  // this stage is read; the next iteration may refill it
+        if (tid == 0) s_next[st] = 0;
     }
 }
 
@@ -1023,6 +1215,7 @@ IndexView view_of(const abf_index* ix) {
     v.term_cbytes = ix->dev.term_cbytes;
     v.dense_stride = ix->derived.dense_stride;
     v.dir_n = ix->derived.dir_n;
+    v.n_dense = ix->derived.n_dense;
     v.n_terms = ix->n_terms;
     v.n_ads = ix->n_ads;
     v.n_blocks = ix->n_blocks;
@@ -1108,6 +1301,74 @@ cudaError_t launch_tile_union(const IndexView& v, const TileArgs& a, const abf_t
     }
     count_launch();
     return e;
+}
+
+namespace {
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encoder() {
+    static EncodeTiledFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return EncodeTiledFn(nullptr);
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return fn;
+}
+}  // namespace
+
+cudaError_t encode_dense_tmap(const IndexView& v, void* out) {
+    static_assert(sizeof(CUtensorMap) == 128, "tensor map size");
+    EncodeTiledFn fn = encoder();
+    if (!fn || !v.dense || v.n_dense == 0) return cudaErrorNotSupported;
+    // dims: words of a bitmap (innermost), bitmaps; rows past n_dense read as
+    // zeros. Two descriptors: boxes of 256 bitmaps, and one box for the rest
+    // plus the zero row, so a stage holds exactly n_dense + 1 rows.
+    const uint32_t rows = v.n_dense + 1u;
+    const uint32_t last = rows - (rows - 1u) / kGroupBoxRows * kGroupBoxRows;
+    const cuuint64_t dims[2] = {cuuint64_t(v.dense_stride), cuuint64_t(v.n_dense)};
+    const cuuint64_t strides[1] = {cuuint64_t(v.dense_stride) * 4u};
+    const cuuint32_t es[2] = {1, 1};
+    for (int k = 0; k < 2; ++k) {
+        const cuuint32_t box[2] = {kGroupTileWords, k == 0 ? kGroupBoxRows : last};
+        const CUresult r = fn(reinterpret_cast<CUtensorMap*>(out) + k, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2,
+                              const_cast<uint32_t*>(v.dense), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    }
+    return cudaSuccess;
+}
+
+uint32_t dense_group_list_cap(uint32_t n_rows, uint32_t n_q) {
+    const uint64_t stage = (uint64_t(n_rows) * kGroupTileWords * 4u + 1023u) & ~1023ull;
+    const uint64_t used = 1024u + 2u * stage + ((6ull * n_q + 15u) & ~15ull);
+    return used >= kGroupSmemBytes ? 0u : uint32_t((kGroupSmemBytes - used) / 2u) & ~7u;
+}
+
+cudaError_t launch_dense_group(const void* tmaps, const DenseGroupArgs& a, int sm_count, cudaStream_t s) {
+    if (a.n_q == 0 || a.n_tiles == 0) return cudaSuccess;
+    if (a.n_rows < 2 || a.n_rows > kGroupMaxBoxes * kGroupBoxRows || a.n_q > kGroupMaxQueries)
+        return cudaErrorInvalidValue;
+    static std::atomic<uint64_t> done{0};  // devices whose attribute is set
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (!(done.load() >> dev & 1ull)) {
+        e = cudaFuncSetAttribute(dense_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(kGroupSmemBytes));
+        if (e != cudaSuccess) return e;
+        done.fetch_or(1ull << dev);
+    }
+    CUtensorMap m[2];
+    std::memcpy(m, tmaps, sizeof(m));
+    const uint32_t grid = a.n_tiles < uint32_t(sm_count) ? a.n_tiles : uint32_t(sm_count);
+    dense_group_kernel<<<grid, kGroupThreads, kGroupSmemBytes, s>>>(m[0], m[1], a);
+    count_launch();
+    return cudaGetLastError();
 }
 
 cudaError_t launch_scatter(const IndexView& v, const ScatterArgs& a, const abf_tuning& t, int sm_count,

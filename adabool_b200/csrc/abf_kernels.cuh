@@ -57,10 +57,14 @@ struct PlanArgs {
     int dense_in_tile;        // 1: dense-bitmap lists go to the merge kernel, 0: scattered too
     uint32_t* tile_cls;       // out: per term slot, what the merge kernel does with it
                               // (kNone: nothing, kDenseFlag | d: dense bitmap d, else the term)
-    uint32_t* q_dense;        // out (optional): per query, its dense bitmap indices packed
-                              // from the query's first term slot on
-    uint32_t* q_ndense;       // out (with q_dense): per query, dense bitmaps to merge
-    uint32_t* q_nmerge;       // out (with q_dense): per query, merged lists without a dense bitmap
+    // optional per-query dense-bitmap lists (all four set, or q_dense16 null):
+    // the query's distinct dense bitmap indices in ascending order, as 16-bit
+    // values from q_dense16 + q_dstart[q] (16-byte aligned), padded to a
+    // multiple of 8 with the index n_dense (an all-zero row for the TMA path)
+    uint16_t* q_dense16;      // out: max_terms + 8 * n_q + 16 entries
+    uint32_t* q_dstart;       // out: per query
+    uint32_t* q_ndense;       // out: per query, distinct dense bitmaps
+    uint32_t* q_dmode;        // out: per query, 1 if every list it merges has a dense bitmap
 };
 
 constexpr uint32_t kDenseFlag = 0x80000000u;
@@ -93,9 +97,37 @@ struct TileArgs {
     uint64_t n_words;         // words of one bitmap
     int accumulate;           // 1: OR into the existing bitmap, 0: overwrite
     int vec_ok;               // out 16-byte aligned and out_stride % 4 == 0
-    const uint32_t* q_dense;  // optional (plan kernel): queries whose merged lists all have
-    const uint32_t* q_ndense; // dense bitmaps take a barrier-free path that streams the OR of
-    const uint32_t* q_nmerge; // their slices straight to the output
+    // optional (plan kernel): queries whose merged lists all have dense
+    // bitmaps (q_dmode) take a barrier-free path that streams the OR of their
+    // slices straight to the output, or are skipped when the dense group
+    // kernel covers them
+    const uint16_t* q_dense16;
+    const uint32_t* q_dstart;
+    const uint32_t* q_ndense;
+    const uint32_t* q_dmode;
+    int skip_dense_only;
+};
+
+// dense group kernel: one pass per 32-word tile over all dense-only queries
+constexpr uint32_t kGroupTileWords = 32;
+constexpr uint32_t kGroupBoxRows = 256;   // dense bitmaps per TMA box
+constexpr uint32_t kGroupMaxBoxes = 3;    // up to 767 dense bitmaps plus the zero row
+constexpr uint32_t kGroupMaxQueries = 2048;
+constexpr uint32_t kGroupSmemBytes = 226u * 1024u;  // dynamic shared memory of the group kernel
+
+struct DenseGroupArgs {
+    const uint16_t* q_dense16;
+    const uint32_t* q_dstart;
+    const uint32_t* q_ndense;
+    const uint32_t* q_dmode;
+    uint32_t n_q;              // <= kGroupMaxQueries
+    uint32_t n_rows;           // n_dense + 1 (the last row reads as zeros)
+    uint32_t list_cap;         // 16-bit list entries that fit in shared memory
+    uint32_t n_tiles;          // ceil(n_words / 32)
+    uint32_t* out;
+    uint64_t out_stride;
+    uint64_t n_words;
+    uint32_t* err;
 };
 
 struct ScatterArgs {
@@ -146,6 +178,13 @@ uint32_t compact_chunks(uint64_t n_bits);
 uint64_t scan_tiles(uint64_t n);
 
 cudaError_t launch_plan(const IndexView& v, const PlanArgs& a, cudaStream_t s);
+// two 2-D TMA descriptors (2 x 128 bytes into out) of the dense bitmaps:
+// 32-word x 256-bitmap boxes, and one box for the remaining bitmaps plus the
+// zero row; cudaErrorNotSupported when the driver has no encoder
+cudaError_t encode_dense_tmap(const IndexView& v, void* out);
+// 16-bit list entries the group kernel can stage in shared memory
+uint32_t dense_group_list_cap(uint32_t n_rows, uint32_t n_q);
+cudaError_t launch_dense_group(const void* tmaps, const DenseGroupArgs& a, int sm_count, cudaStream_t s);
 cudaError_t launch_queue_scan(const QueueArgs& a, cudaStream_t s);
 cudaError_t launch_probe_bits(const ProbeBitsArgs& a, uint32_t probe_cap, cudaStream_t s);
 cudaError_t launch_tile_union(const IndexView& v, const TileArgs& a, const abf_tuning& t, int sm_count,

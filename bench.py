@@ -297,6 +297,15 @@ def run_ours(args, rank, world, dev):
         "compact_count": n_q * bm_bytes,
         "compact_write": n_q * bm_bytes + 4.0 * float(counts.sum()),
     }
+    if "dense_group" in kern:
+        # the group kernel reads every dense bitmap once per launch and writes
+        # the bitmaps of the queries whose merged lists are all dense; the
+        # merge kernel keeps the others
+        n_dense = int(dense_t.sum())
+        dense_only = (per_query((merged_t & ~dense_t)[qterms].astype(np.float64)) == 0) & ~empty
+        alg["dense_group"] = kern["dense_group"][0] / args.steps * n_dense * bm_bytes + \
+            float(dense_only.sum()) * bm_bytes
+        alg["tile_union"] = float(np.sum(q_merge[~dense_only])) + float((~dense_only).sum()) * bm_bytes
     total_alg = float(np.sum(q_all)) + 16.0 * qterms.size + 2 * n_q * bm_bytes + 4.0 * float(counts.sum())
     hbm, peak_kind = peaks()
     per_kernel = {}

@@ -150,6 +150,11 @@ typedef struct abf_tuning {
     float probe_min_fraction; /* fixed rule (ABF_PATH_AUTO without a planner): probe
                                  when the query's lists hold more than this fraction
                                  of all blocks, else list-union */
+    uint32_t group_min_queries; /* batches of at least this many queries merge the
+                                 dense bitmaps of all their dense-only queries in one
+                                 pass per 32-word tile (each tile's slice of every dense
+                                 bitmap staged once in shared memory by TMA, then ORed
+                                 per query); needs at most 767 dense bitmaps; 0 = never */
 } abf_tuning;
 
 abf_status abf_get_tuning(const abf_index* index, abf_tuning* out);

@@ -112,6 +112,46 @@ def test_batch_mixed_paths_and_probe_overflow(small):
         ix.set_tuning(probe_cap=old)
 
 
+@pytest.mark.parametrize("dense_div", [16, 128, 512, 4096])
+@pytest.mark.parametrize("path", [ab.PATH_UNION, ab.PATH_HYBRID, ab.PATH_AUTO, "mixed"])
+def test_dense_group_kernel(small, dense_div, path):
+    """The dense group kernel (one pass per 32-word tile over every
+    dense-only query, dense slices staged by TMA) against the oracle, on and
+    off, with 1, 2 or 3 TMA boxes of dense bitmaps or too many for it."""
+    torch = _torch()
+    ix, n_words, qs = small["ix"], small["n_words"], small["qs"]
+    old_dd, old_gm = ix.dense_div, ix.tuning.group_min_queries
+    qoff = np.zeros(len(qs) + 1, np.uint64)
+    qoff[1:] = np.cumsum([q.size for q in qs])
+    flat = np.concatenate(qs).astype(np.uint32)
+    d_terms = torch.from_numpy(flat.view(np.int32)).cuda()
+    d_off = torch.from_numpy(qoff.view(np.int64)).cuda()
+    d_paths = None
+    if path == "mixed":
+        paths = np.random.default_rng(11).choice([1, 2, 3, 4, 0], size=len(qs)).astype(np.uint8)
+        d_paths = torch.from_numpy(paths).cuda()
+    stride = ((n_words + 3) // 4) * 4
+    expect = [expected(small["off"], small["ads"], q, n_words)[1] for q in qs]
+    try:
+        ix.set_dense_div(dense_div)
+        n_dense = ix.stats()["n_dense_lists"]
+        ws = ix.workspace(len(qs), int(qoff[-1]) + 1)
+        for gm in (0, 1):
+            ix.set_tuning(group_min_queries=gm)
+            bms = torch.full((len(qs), stride), -1, dtype=torch.int32, device="cuda")
+            ix.batch_run(ws, d_terms, d_off, len(qs), bms, stride, path=0 if path == "mixed" else path,
+                         d_paths=d_paths)
+            ws.check()
+            got = bms.cpu().numpy().view(np.uint32)
+            for i in range(len(qs)):
+                assert np.array_equal(got[i, :n_words], expect[i]), \
+                    f"query {i}, dense_div {dense_div} ({n_dense} dense), group {gm}, path {path}"
+        ws.free()
+    finally:
+        ix.set_dense_div(old_dd)
+        ix.set_tuning(group_min_queries=old_gm)
+
+
 @pytest.mark.parametrize("tile_words", [256, 512, 1024, 4096, 16384])
 @pytest.mark.parametrize("warps", [1, 2, 4, 8])
 def test_tuning_sweep_identical(small, tile_words, warps):
