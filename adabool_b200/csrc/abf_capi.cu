@@ -487,8 +487,7 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
     // 32-word tile, when the batch is large enough and the dense bitmaps
     // (plus the zero row) fit three TMA boxes of 256
     const uint32_t n_dense = v.n_dense;
-    bool group = t.group_min_queries && b->n_queries >= t.group_min_queries &&
-                 b->n_queries <= abf::kGroupMaxQueries && n_dense > 0 &&
+    bool group = t.group_min_queries && b->n_queries >= t.group_min_queries && n_dense > 0 &&
                  n_dense + 1 <= abf::kGroupMaxBoxes * abf::kGroupBoxRows;
     if (group && (ix->dense_tmap_base != ix->dev.dense || ix->dense_tmap_rows != n_dense)) {
         if (abf::encode_dense_tmap(v, ix->dense_tmap) == cudaSuccess) {
@@ -499,17 +498,19 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
         }
     }
     ta.skip_dense_only = group ? 1 : 0;
-    if (group) {
+    // one launch per window of at most kGroupMaxQueries queries (their
+    // per-query state must fit the kernel's shared memory)
+    for (uint32_t q0 = 0; group && q0 < b->n_queries; q0 += abf::kGroupMaxQueries) {
         abf::DenseGroupArgs ga{};
         ga.q_dense16 = ws->q_dense16;
-        ga.q_dstart = ws->q_dstart;
-        ga.q_ndense = ws->q_ndense;
-        ga.q_dmode = ws->q_dmode;
-        ga.n_q = b->n_queries;
+        ga.q_dstart = ws->q_dstart + q0;
+        ga.q_ndense = ws->q_ndense + q0;
+        ga.q_dmode = ws->q_dmode + q0;
+        ga.n_q = std::min<uint32_t>(abf::kGroupMaxQueries, b->n_queries - q0);
         ga.n_rows = n_dense + 1;
-        ga.list_cap = abf::dense_group_list_cap(ga.n_rows, b->n_queries);
+        ga.list_cap = abf::dense_group_list_cap(ga.n_rows, ga.n_q);
         ga.n_tiles = uint32_t((n_words + abf::kGroupTileWords - 1) / abf::kGroupTileWords);
-        ga.out = b->d_bitmaps;
+        ga.out = b->d_bitmaps + uint64_t(q0) * b->bitmap_stride_words;
         ga.out_stride = b->bitmap_stride_words;
         ga.n_words = n_words;
         ga.err = ws->err;

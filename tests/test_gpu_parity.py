@@ -152,6 +152,37 @@ def test_dense_group_kernel(small, dense_div, path):
         ix.set_tuning(group_min_queries=old_gm)
 
 
+def test_dense_group_windows(small):
+    """Batches above 2,048 queries run the dense group kernel window by
+    window; every bitmap equals the merge kernel's and, on a sample, the
+    oracle's."""
+    torch = _torch()
+    ix, n_words, spec = small["ix"], small["n_words"], small["spec"]
+    lens = np.diff(small["off"]).astype(np.uint32)
+    qoff, qt = W.gen_queries(W.QueriesSpec(2300, "lognormal", 6.0, 1.5, 1, 200, seed=19), lens)
+    n = qoff.size - 1
+    stride = ((n_words + 3) // 4) * 4
+    d_terms = torch.from_numpy(qt.astype(np.uint32).view(np.int32)).cuda()
+    d_off = torch.from_numpy(qoff.astype(np.uint64).view(np.int64)).cuda()
+    ws = ix.workspace(n, int(qoff[-1]) + 1)
+    old_gm = ix.tuning.group_min_queries
+    out = []
+    try:
+        for gm in (0, 1):
+            ix.set_tuning(group_min_queries=gm)
+            bms = torch.full((n, stride), -1, dtype=torch.int32, device="cuda")
+            ix.batch_run(ws, d_terms, d_off, n, bms, stride, path=ab.PATH_UNION)
+            ws.check()
+            out.append(bms[:, :n_words].cpu().numpy().view(np.uint32))
+    finally:
+        ix.set_tuning(group_min_queries=old_gm)
+        ws.free()
+    assert np.array_equal(out[0], out[1])
+    for i in list(range(0, n, 97)) + [2047, 2048, n - 1]:
+        q = qt[qoff[i]:qoff[i + 1]]
+        assert np.array_equal(out[1][i], expected(small["off"], small["ads"], q, n_words)[1]), f"query {i}"
+
+
 @pytest.mark.parametrize("tile_words", [256, 512, 1024, 4096, 16384])
 @pytest.mark.parametrize("warps", [1, 2, 4, 8])
 def test_tuning_sweep_identical(small, tile_words, warps):
