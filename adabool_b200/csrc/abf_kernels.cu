@@ -992,20 +992,39 @@ __device__ __forceinline__ uint32_t masked_word(const uint32_t* bm, uint64_t w, 
     return v;
 }
 
+// Set bits per 2048-word chunk. A full, 16-byte aligned chunk is read with
+// two 16-byte loads per thread; the warps' sums meet in a shared array
+// double-buffered by chunk parity, so a chunk costs one barrier.
 __global__ void __launch_bounds__(256) count_kernel(CompactArgs a) {
-    __shared__ unsigned long long s_red[8];
+    static_assert(kCompactChunkWords == 256 * 8, "two uint4 per thread");
+    __shared__ uint32_t s_red[2][8];
+    const uint32_t tid = threadIdx.x, lane = lane_id(), warp = warp_id();
     const uint64_t n_words = (a.n_bits + 31) / 32;
     const uint64_t items = uint64_t(a.n_q) * a.n_chunks;
-    for (uint64_t item = blockIdx.x; item < items; item += gridDim.x) {
+    uint32_t parity = 0;
+    for (uint64_t item = blockIdx.x; item < items; item += gridDim.x, parity ^= 1u) {
         const uint32_t q = uint32_t(item / a.n_chunks);
         const uint32_t c = uint32_t(item - uint64_t(q) * a.n_chunks);
         const uint32_t* bm = a.bm + uint64_t(q) * a.stride;
         const uint64_t w0 = uint64_t(c) * kCompactChunkWords;
-        const uint64_t w1 = w0 + kCompactChunkWords < n_words ? w0 + kCompactChunkWords : n_words;
-        uint64_t s = 0;
-        for (uint64_t w = w0 + threadIdx.x; w < w1; w += 256) s += __popc(masked_word(bm, w, a.n_bits));
-        s = block_sum_u64<256>(s, s_red);
-        if (threadIdx.x == 0) a.counts[item] = uint32_t(s);
+        uint32_t s = 0;
+        if ((w0 + kCompactChunkWords) * 32u <= a.n_bits && (reinterpret_cast<uintptr_t>(bm + w0) & 15u) == 0) {
+            const uint4* p = reinterpret_cast<const uint4*>(bm + w0);
+            const uint4 x0 = p[tid], x1 = p[tid + 256u];
+            s = __popc(x0.x) + __popc(x0.y) + __popc(x0.z) + __popc(x0.w) + __popc(x1.x) + __popc(x1.y) +
+                __popc(x1.z) + __popc(x1.w);
+        } else {
+            const uint64_t w1 = w0 + kCompactChunkWords < n_words ? w0 + kCompactChunkWords : n_words;
+            for (uint64_t w = w0 + tid; w < w1; w += 256) s += __popc(masked_word(bm, w, a.n_bits));
+        }
+        s = __reduce_add_sync(kFull, s);
+        if (lane == 0) s_red[parity][warp] = s;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t t = lane < 8u ? s_red[parity][lane] : 0u;
+            t = __reduce_add_sync(kFull, t);
+            if (lane == 0) a.counts[item] = t;
+        }
     }
 }
 
