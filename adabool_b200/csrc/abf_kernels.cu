@@ -662,26 +662,30 @@ __device__ __forceinline__ uint32_t or_list(const uint32_t* S, const uint4* dl, 
     return acc;
 }
 
-// OR over a list staged in shared memory as byte offsets of rows (row * 128),
-// 8 at a time: one add, one load and half a 3-input OR per row
-__device__ __forceinline__ uint32_t or_list_bytes(const uint8_t* B, const uint4* ol, uint32_t nd) {
-    uint32_t acc = 0;
-    for (uint32_t k = 0; k < nd; k += 8u) {
-        const uint4 a = ol[k >> 2], b = ol[(k >> 2) + 1];
-        acc |= (*reinterpret_cast<const uint32_t*>(B + a.x) | *reinterpret_cast<const uint32_t*>(B + a.y) |
-                *reinterpret_cast<const uint32_t*>(B + a.z)) |
-               (*reinterpret_cast<const uint32_t*>(B + a.w) | *reinterpret_cast<const uint32_t*>(B + b.x) |
-                *reinterpret_cast<const uint32_t*>(B + b.y)) |
-               (*reinterpret_cast<const uint32_t*>(B + b.z) | *reinterpret_cast<const uint32_t*>(B + b.w));
-    }
+// OR over a list staged in shared memory as 16-bit word offsets of rows
+// (row * 32), 8 per 16-byte load: per row one extract, one address, one
+// shared load and half a 3-input OR
+__device__ __forceinline__ uint32_t ld_row(const uint8_t* B, uint32_t woff) {
+    return *reinterpret_cast<const uint32_t*>(B + (woff << 2));
+}
+__device__ __forceinline__ uint32_t or8w(const uint8_t* B, uint4 v) {
+    return (ld_row(B, v.x & 0xffffu) | ld_row(B, v.x >> 16) | ld_row(B, v.y & 0xffffu)) |
+           (ld_row(B, v.y >> 16) | ld_row(B, v.z & 0xffffu) | ld_row(B, v.z >> 16)) |
+           (ld_row(B, v.w & 0xffffu) | ld_row(B, v.w >> 16));
+}
+__device__ __forceinline__ uint32_t or_list_words(const uint8_t* B, const uint4* ol, uint32_t nd) {
+    uint32_t acc = 0, k = 0;
+    for (; k + 16u <= nd; k += 16u) acc |= or8w(B, ol[k >> 3]) | or8w(B, ol[(k >> 3) + 1]);
+    if (k < nd) acc |= or8w(B, ol[k >> 3]);
+    if (k + 8u < nd) acc |= or8w(B, ol[(k >> 3) + 1]);
     return acc;
 }
 
 // Shared memory (dynamic, 1024-byte aligned base): two stages of n_rows x
 // 32 words (rows = dense bitmaps + the zero row), then per dense-only query
 // its list's offset and length, the queue of dense-only queries, and the
-// lists themselves as 32-bit row byte offsets when they fit (else the 16-bit
-// row lists are read from global memory).
+// lists themselves as 16-bit row word offsets when they fit (else the
+// 16-bit row lists are read from global memory).
 __global__ void __launch_bounds__(kGroupThreads, 1)
     dense_group_kernel(const __grid_constant__ CUtensorMap tmap_full, const __grid_constant__ CUtensorMap tmap_last,
                        DenseGroupArgs a) {
@@ -695,7 +699,7 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
     uint32_t* stage0 = reinterpret_cast<uint32_t*>(base);
     uint32_t* s_meta = reinterpret_cast<uint32_t*>(base + 2u * stage_bytes);  // n_q: list offset / 8 << 16 | nd
     uint16_t* s_qlist = reinterpret_cast<uint16_t*>(s_meta + a.n_q);          // dense-only queries
-    uint4* s_lists = reinterpret_cast<uint4*>(base + 2u * stage_bytes + ((6u * a.n_q + 15u) & ~15u));  // 4 offsets each
+    uint4* s_lists = reinterpret_cast<uint4*>(base + 2u * stage_bytes + ((6u * a.n_q + 15u) & ~15u));  // 8 offsets each
     const uint32_t tid = threadIdx.x, lane = lane_id(), warp = warp_id();
     constexpr uint32_t kNW = kGroupThreads / 32u;
     uint32_t t = blockIdx.x;
@@ -751,14 +755,12 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
             const uint32_t q = s_qlist[i];
             const uint32_t m = s_meta[q];
             const uint4* src = reinterpret_cast<const uint4*>(a.q_dense16 + a.q_dstart[q]);
-            uint4* dst = s_lists + (m >> 16) * 2u;  // 8 entries = two uint4 of byte offsets
-            constexpr uint32_t kRowBytes = kGroupTileWords * 4u;
+            uint4* dst = s_lists + (m >> 16);
+            // rows -> word offsets (row * 32 < 2^15: both halves shift together)
+            static_assert(kGroupTileWords == 32u && kGroupMaxBoxes * kGroupBoxRows * 32u < 65536u, "offsets");
             for (uint32_t j = lane; j < ((m & 0xffffu) + 7u) / 8u; j += 32u) {
                 const uint4 v = src[j];
-                dst[2u * j] = make_uint4((v.x & 0xffffu) * kRowBytes, (v.x >> 16) * kRowBytes,
-                                         (v.y & 0xffffu) * kRowBytes, (v.y >> 16) * kRowBytes);
-                dst[2u * j + 1u] = make_uint4((v.z & 0xffffu) * kRowBytes, (v.z >> 16) * kRowBytes,
-                                              (v.w & 0xffffu) * kRowBytes, (v.w >> 16) * kRowBytes);
+                dst[j] = make_uint4(v.x << 5, v.y << 5, v.z << 5, v.w << 5);
             }
         }
     }
@@ -798,7 +800,7 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
             const uint32_t m = s_meta[q];
             const uint32_t nd = m & 0xffffu;
             const uint32_t acc =
-                in_smem ? or_list_bytes(B, s_lists + (m >> 16) * 2u, nd)
+                in_smem ? or_list_words(B, s_lists + (m >> 16), nd)
                         : or_list(S, reinterpret_cast<const uint4*>(a.q_dense16 + a.q_dstart[q]), nd, lane);
             if (w < a.n_words) a.out[uint64_t(q) * a.out_stride + w] = acc;
         }
@@ -1390,7 +1392,7 @@ cudaError_t encode_dense_tmap(const IndexView& v, void* out) {
 uint32_t dense_group_list_cap(uint32_t n_rows, uint32_t n_q) {
     const uint64_t stage = (uint64_t(n_rows) * kGroupTileWords * 4u + 1023u) & ~1023ull;
     const uint64_t used = 1024u + 2u * stage + ((6ull * n_q + 15u) & ~15ull);
-    return used >= kGroupSmemBytes ? 0u : uint32_t((kGroupSmemBytes - used) / 4u) & ~7u;
+    return used >= kGroupSmemBytes ? 0u : uint32_t((kGroupSmemBytes - used) / 2u) & ~7u;
 }
 
 cudaError_t launch_dense_group(const void* tmaps, const DenseGroupArgs& a, int sm_count, cudaStream_t s) {

@@ -122,7 +122,7 @@ struct DenseGroupArgs {
     const uint32_t* q_dmode;
     uint32_t n_q;              // <= kGroupMaxQueries
     uint32_t n_rows;           // n_dense + 1 (the last row reads as zeros)
-    uint32_t list_cap;         // list entries (32-bit row offsets) that fit in shared memory
+    uint32_t list_cap;         // list entries (16-bit row word offsets) that fit in shared memory
     uint32_t n_tiles;          // ceil(n_words / 32)
     uint32_t* out;
     uint64_t out_stride;
@@ -182,7 +182,7 @@ cudaError_t launch_plan(const IndexView& v, const PlanArgs& a, cudaStream_t s);
 // 32-word x 256-bitmap boxes, and one box for the remaining bitmaps plus the
 // zero row; cudaErrorNotSupported when the driver has no encoder
 cudaError_t encode_dense_tmap(const IndexView& v, void* out);
-// list entries (32-bit row offsets) the group kernel can stage in shared memory
+// list entries (16-bit row word offsets) the group kernel can stage in shared memory
 uint32_t dense_group_list_cap(uint32_t n_rows, uint32_t n_q);
 cudaError_t launch_dense_group(const void* tmaps, const DenseGroupArgs& a, int sm_count, cudaStream_t s);
 cudaError_t launch_queue_scan(const QueueArgs& a, cudaStream_t s);
