@@ -62,6 +62,8 @@ def parse():
     p.add_argument("--path", default="hybrid", choices=["auto", "probe", "union", "hybrid", "tile", "planner"])
     p.add_argument("--no-autotune", action="store_true", help="keep the library's default tuning")
     p.add_argument("--tuning", default="", help="apply a saved autotuner result (JSON) instead of tuning")
+    p.add_argument("--tuning-set", default="",
+                   help="explicit knobs instead of tuning, e.g. dense_div=256,tile_words=16384,group_min_queries=32")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -101,10 +103,16 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # nvidia-smi takes a moment to start: the timed region begins once
+            # it has produced its first sample, and only later ones count
+            t_end = time.time() + 5.0
+            while not self.lines and time.time() < t_end and self.proc.poll() is None:
+                time.sleep(0.01)
+            self.start = len(self.lines)
         except Exception:
             self.proc = None
         return self
@@ -124,7 +132,8 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        during = self.lines[getattr(self, "start", 0):] or self.lines[-1:]
+        for ln in during:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 8:
                 continue
@@ -186,7 +195,12 @@ def run_ours(args, rank, world, dev):
     path = {"auto": ab.PATH_AUTO, "probe": ab.PATH_PROBE, "union": ab.PATH_UNION, "hybrid": ab.PATH_HYBRID,
             "tile": ab.PATH_TILE, "planner": ab.PATH_AUTO}[args.path]
     tune_info = None
-    if args.tuning:
+    if args.tuning_set:
+        from adabool_b200 import autotune as AT
+        kv = dict(x.split("=", 1) for x in args.tuning_set.split(",") if x)
+        AT.apply(ix, {k: (float(v) if k == "probe_min_fraction" else int(v)) for k, v in kv.items()})
+        tune_info = {"set": args.tuning_set}
+    elif args.tuning:
         from adabool_b200 import autotune as AT
         AT.apply(ix, args.tuning)
         tune_info = {"from": args.tuning}
