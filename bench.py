@@ -10,10 +10,16 @@ bitmap (2^24 bits) plus sorted uint32 id list per query, through the batched
 API in sub-batches. Inputs are larger than L2 (the compressed index alone is
 ~0.8 GB), so no flush is needed between steps.
 
-  value  queries/s with inputs already in HBM (device-timed, CUDA events)
+  value  queries/s with inputs already in HBM (device-timed, CUDA events);
+         sub-batches alternate over --streams streams, each with its own
+         workspace and output buffers
   e2e    the same through the public API from pinned host buffers: per
          sub-batch the query terms go host->device and every id list comes
          back device->host inside the timed region
+  roofline / kernels
+         per-kernel CUDA-event durations from the same steps run once more
+         on a single stream (no overlap), against the algorithmic bytes of
+         each kernel
 
 Multi-GPU: replicas (each rank its own query set on its own copy of the
 index, no collective on the data path), launched by torchrun; the time is
@@ -57,6 +63,8 @@ def parse():
     p.add_argument("--config", default="c1")
     p.add_argument("--scale", type=float, default=1.0, help="shrink the workload (profiling / quick runs)")
     p.add_argument("--queries", type=int, default=0, help="override the query count")
+    p.add_argument("--streams", type=int, default=2,
+                   help="streams the sub-batches alternate over (each with its own workspace and buffers)")
     p.add_argument("--sub-batch", type=int, default=0,
                    help="queries per abf_batch_run call (0: tuned among 128/256/512, 256 without the tuner)")
     p.add_argument("--path", default="hybrid", choices=["auto", "probe", "union", "hybrid", "tile", "planner"])
@@ -231,17 +239,30 @@ def run_ours(args, rank, world, dev):
     # device-resident inputs per sub-batch
     d_in = [(torch.from_numpy(t.view(np.int32)).to(dev) if t.size else torch.zeros(1, dtype=torch.int32, device=dev),
              torch.from_numpy(o.view(np.int64)).to(dev), b - a) for a, b, o, t in sbs]
-    nbuf = 1 if args.no_e2e else 2
+    n_streams = max(1, min(args.streams, len(sbs)))
+    nbuf = max(n_streams, 1 if args.no_e2e else 2)
     ws = [ix.workspace(sbq, max_terms) for _ in range(nbuf)]
     bms = [torch.empty((sbq, stride), dtype=torch.int32, device=dev) for _ in range(nbuf)]
     ids = [torch.empty(cap, dtype=torch.int32, device=dev) for _ in range(nbuf)]
     idoff = [torch.zeros(sbq + 1, dtype=torch.int64, device=dev) for _ in range(nbuf)]
     stream = torch.cuda.Stream(device=dev)
+    streams = [stream] + [torch.cuda.Stream(device=dev) for _ in range(n_streams - 1)]
+    fork = torch.cuda.Event()
+    joins = [torch.cuda.Event() for _ in streams]
 
     def step():
-        for (dt, do, nq) in d_in:
-            ix.batch_run(ws[0], dt, do, nq, bms[0], stride, path=path, d_ids=ids[0], d_id_offsets=idoff[0],
-                         stream=stream)
+        # sub-batch i runs on stream i % n with buffer set i % n, so one
+        # sub-batch's compaction overlaps the next one's merge and scatter
+        fork.record(stream)
+        for s in streams[1:]:
+            s.wait_event(fork)
+        for i, (dt, do, nq) in enumerate(d_in):
+            k = i % n_streams
+            ix.batch_run(ws[k], dt, do, nq, bms[k], stride, path=path, d_ids=ids[k], d_id_offsets=idoff[k],
+                         stream=streams[k])
+        for s, e in zip(streams[1:], joins[1:]):
+            e.record(s)
+            stream.wait_event(e)
 
     # correctness spot check + result sizes (untimed)
     with torch.cuda.stream(stream):
@@ -257,9 +278,6 @@ def run_ours(args, rank, world, dev):
     for _ in range(args.warmup):
         step()
     stream.synchronize()
-    dist_barrier(world)
-    ix.profile(True)
-    ix.profile_read()
     n_launch0 = ab.launch_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize(dev)
@@ -273,10 +291,21 @@ def run_ours(args, rank, world, dev):
     torch.cuda.synchronize(dev)
     launches = (ab.launch_count() - n_launch0) // max(args.steps, 1)
     ms_total = e0.elapsed_time(e1)
-    kern = ix.profile_read()
-    ix.profile(False)
     ms_step = dist_max(ms_total / args.steps, world)
     dist_barrier(world)
+
+    # per-kernel CUDA-event times for the roofline: the same K steps once
+    # more on one stream, so no kernel's duration includes another's
+    # contention (in the timed region they overlap across streams)
+    ix.profile(True)
+    ix.profile_read()
+    for _ in range(args.steps):
+        for (dt, do, nq) in d_in:
+            ix.batch_run(ws[0], dt, do, nq, bms[0], stride, path=path, d_ids=ids[0], d_id_offsets=idoff[0],
+                         stream=stream)
+    stream.synchronize()
+    kern = ix.profile_read()
+    ix.profile(False)
 
     # ---- e2e through the public API from pinned host buffers ----
     e2e = None
@@ -343,7 +372,9 @@ def run_ours(args, rank, world, dev):
                 "frac": round(a / hbm, 4), "peak_kind": peak_kind, "traffic": traffic,
                 "alg_bytes_per_launch": round(alg[dom] / n_launch),
                 "traffic_source": None if ratio is None else
-                "ncu capture of this kernel at 1/4 scale (profiles/), scaled by the ids a launch writes"}
+                "ncu capture of this kernel at 1/4 scale (profiles/), scaled by the ids a launch writes",
+                "duration_source": "CUDA events around each launch in a single-stream pass of the same steps "
+                                   "right after the timed region"}
     postings = float(np.sum(qpost))
     value = n_q * world / (ms_step / 1e3)
     res = {
@@ -351,7 +382,7 @@ def run_ours(args, rank, world, dev):
         "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded Zipf lists, lognormal queries)",
         "config": {"workload": f"{cfg.name}: {L.n_terms} terms x {L.n_ads} ads, {st['n_postings']} postings; "
-                               f"{n_q} queries/rank, sub-batches of {args.sub_batch}",
+                               f"{n_q} queries/rank, sub-batches of {args.sub_batch} on {n_streams} streams",
                    "path": args.path, "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (no flush)",
                    "index_bytes": ix.stats()["device_bytes"],
                    "tuning": dict(ix.tuning.as_dict(), dense_div=ix.dense_div), "autotune": tune_info},
