@@ -57,7 +57,7 @@ def apply(index, path_or_dict):
 
 
 class _Runner:
-    def __init__(self, index, q_off, q_terms, sub_batch, path, device):
+    def __init__(self, index, q_off, q_terms, sub_batch, path, device, n_streams: int = 1):
         import torch
         self.torch = torch
         self.ix = index
@@ -74,22 +74,40 @@ class _Runner:
             self.sbs.append((dt, torch.from_numpy(o.view(np.int64)).to(device), b - a))
         mq = max(s[2] for s in self.sbs)
         mt = max(int(s[0].numel()) for s in self.sbs) + 1
-        self.ws = index.workspace(mq, mt)
-        self.bms = torch.empty((mq, self.stride), dtype=torch.int32, device=device)
-        self.stream = torch.cuda.Stream(device=device)
+        n = max(1, min(n_streams, len(self.sbs)))
+        # sub-batch i runs on stream i % n with its own workspace and bitmaps
+        self.wss = [index.workspace(mq, mt) for _ in range(n)]
+        self.ws = self.wss[0]
+        self.bms = [torch.empty((mq, self.stride), dtype=torch.int32, device=device) for _ in range(n)]
+        self.streams = [torch.cuda.Stream(device=device) for _ in range(n)]
+        self.stream = self.streams[0]
+
+    def _pass(self):
+        for i, (dt, do, nq) in enumerate(self.sbs):
+            k = i % len(self.streams)
+            self.ix.batch_run(self.wss[k], dt, do, nq, self.bms[k], self.stride, path=self.path,
+                              stream=self.streams[k])
 
     def time_ms(self, reps: int) -> float:
         torch = self.torch
-        for dt, do, nq in self.sbs:  # warm-up (also rebuilds nothing: tuning is read per launch)
-            self.ix.batch_run(self.ws, dt, do, nq, self.bms, self.stride, path=self.path, stream=self.stream)
+        self._pass()  # warm-up (tuning is read per launch: nothing to rebuild)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(self.stream)
+        for s in self.streams[1:]:
+            s.wait_event(e0)
         for _ in range(reps):
-            for dt, do, nq in self.sbs:
-                self.ix.batch_run(self.ws, dt, do, nq, self.bms, self.stride, path=self.path, stream=self.stream)
+            self._pass()
+        for s in self.streams[1:]:
+            ev = torch.cuda.Event()
+            ev.record(s)
+            self.stream.wait_event(ev)
         e1.record(self.stream)
         e1.synchronize()
         return e0.elapsed_time(e1) / reps
+
+    def free(self):
+        for w in self.wss:
+            w.free()
 
 
 # knobs that interact, searched jointly: which lists are dense decides which
@@ -175,18 +193,20 @@ def autotune(index, q_off: np.ndarray, q_terms: np.ndarray, path: int = N.PATH_H
 
 
 def tune_sub_batch(index, q_off: np.ndarray, q_terms: np.ndarray, path: int = N.PATH_HYBRID,
-                   candidates=(128, 256, 512, 1024), sample: int = 2048, reps: int = 2, device: int = 0) -> dict:
+                   candidates=(128, 256, 512, 1024), sample: int = 2048, reps: int = 2, device: int = 0,
+                   n_streams: int = 1) -> dict:
     """Queries per abf_batch_run call: larger batches let co-resident merge
     tiles of different queries share L2, smaller ones keep the scatter's
-    working set small. Times each candidate on the same sample."""
+    working set small and give the streams more calls to overlap. Times
+    each candidate on the same sample, calls alternating over n_streams."""
     n = min(sample, q_off.size - 1)
     out = {}
     for sb in candidates:
         if sb > n:
             continue
-        run = _Runner(index, q_off[:n + 1], q_terms[:q_off[n]], sb, path, device)
+        run = _Runner(index, q_off[:n + 1], q_terms[:q_off[n]], sb, path, device, n_streams)
         out[sb] = run.time_ms(reps)
-        run.ws.free()
+        run.free()
         del run
     best = min(out, key=out.get)
     return {"best": best, "ms": out}

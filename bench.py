@@ -220,7 +220,8 @@ def run_ours(args, rank, world, dev):
         tr = AT.autotune(ix, qoff, qterms, path=path, sub_batch=args.sub_batch or 256, sample=1024, device=dev)
         tune_info = {"trials": len(tr.trials), "sample_ms": round(tr.best_ms, 3), "dense_div": tr.best.get("dense_div")}
         if not args.sub_batch:
-            sbt = AT.tune_sub_batch(ix, qoff, qterms, path=path, candidates=(128, 256, 512), device=dev)
+            sbt = AT.tune_sub_batch(ix, qoff, qterms, path=path, candidates=(128, 256, 512), device=dev,
+                                    n_streams=args.streams)
             args.sub_batch = sbt["best"]
             tune_info["sub_batch_ms"] = {str(k): round(v, 3) for k, v in sbt["ms"].items()}
         tune_info["seconds"] = round(time.time() - t0, 1)
