@@ -189,6 +189,7 @@ def autotune(index, q_off: np.ndarray, q_terms: np.ndarray, path: int = N.PATH_H
     apply_cur()
     if "dense_div" in space:
         index.dense_div = cur["dense_div"]
+    run.free()
     return TuneResult(best=dict(cur), best_ms=best_ms, trials=trials)
 
 
