@@ -21,6 +21,18 @@ from .executor import GraphBatchExecutor
 from .index import Index
 
 
+def _autotune_union(ix, cfg, lens, sub_batch, device):
+    """The kernels' tuning for this index (dense threshold, tile width, dense
+    group kernel, ...) from the autotuner on 1,024 seeded queries of the
+    config's shape, timed on the list-union path."""
+    from . import autotune as AT
+    q = W.QueriesSpec(1024, cfg.queries.kind, cfg.queries.median, cfg.queries.sigma, cfg.queries.lo,
+                      cfg.queries.hi, seed=cfg.queries.seed + 104729)
+    qoff, qt = W.gen_queries(q, lens)
+    tr = AT.autotune(ix, qoff, qt, path=N.PATH_UNION, sub_batch=min(sub_batch, 1024), sample=1024, device=device)
+    return dict(tr.best)
+
+
 def _chunked_features(ix, qoff, qt, chunk, device):
     """Features computed in batches of `chunk` queries (the inference batch
     size), so batch-position features mean the same at training time."""
@@ -54,10 +66,11 @@ def planner_experiment(n_train: int = 66_667, batch_config: str = "c2", reps: in
     lens = np.diff(off).astype(np.uint32)
     ix = Index.from_csr(off, ads, L.n_terms, L.n_ads, device=device)
     del off, ads
-    # HYBRID merges per tile every list of at least n_ads/1024 postings (UNION
-    # merges only the dense-bitmap lists), so the three paths differ
     B = cfg.queries.n_queries
-    # probe slots for a whole batch, so PROBE labels really run the probe
+    tuned = _autotune_union(ix, cfg, lens, min(B, 2048), device)
+    # HYBRID merges per tile every list of at least n_ads/1024 postings (UNION
+    # merges only the dense-bitmap lists), so the three paths differ; probe
+    # slots for a whole batch, so PROBE labels really run the probe
     ix.set_tuning(heavy_min_len=max(128, L.n_ads // 1024), probe_cap=B)
     # --- training labels on fresh queries ---
     tq = W.QueriesSpec(n_train, cfg.queries.kind, cfg.queries.median, cfg.queries.sigma, cfg.queries.lo,
@@ -159,7 +172,7 @@ def planner_experiment(n_train: int = 66_667, batch_config: str = "c2", reps: in
         "path_share": {"planner": np.bincount(choice_pl, minlength=3).tolist(),
                        "fixed_rule": np.bincount(choice_fx, minlength=3).tolist(),
                        "best": np.bincount(e_lab.argmin(1), minlength=3).tolist()},
-        "tuning": dict(ix.tuning.as_dict(), dense_div=ix.dense_div),
+        "tuning": dict(ix.tuning.as_dict(), dense_div=ix.dense_div), "autotuned_union": tuned,
         "seconds": round(time.time() - t_start, 1), "params": tr.params,
     }
 
@@ -194,6 +207,7 @@ def serving_experiment(rates=(20_000, 50_000, 100_000, 200_000), offered_seconds
     lens = np.diff(off).astype(np.uint32)
     ix = Index.from_csr(off, ads, L.n_terms, L.n_ads, device=device)
     del off, ads
+    tuned = _autotune_union(ix, cfg, lens, 256, device)
     ix.set_tuning(heavy_min_len=max(128, L.n_ads // 1024), probe_cap=max_batch_queries)
     # --- planner and fixed-rule threshold from batched timing labels ---
     tq = W.QueriesSpec(n_train, cfg.queries.kind, cfg.queries.median, cfg.queries.sigma, cfg.queries.lo,
@@ -265,7 +279,7 @@ def serving_experiment(rates=(20_000, 50_000, 100_000, 200_000), offered_seconds
             "n_streams": n_streams, "fixed_rule_tau": tau,
             "planner_train": {"queries": n_train, "groups": list(label_groups), "samples": int(Y.shape[0]),
                               "val_mse": tr.val_loss, "seconds": round(train_s, 1)},
-            "runs": runs, "tuning": dict(ix.tuning.as_dict(), dense_div=ix.dense_div),
+            "runs": runs, "tuning": dict(ix.tuning.as_dict(), dense_div=ix.dense_div), "autotuned_union": tuned,
             "seconds": round(time.time() - t_start, 1), "params": tr.params}
 
 
