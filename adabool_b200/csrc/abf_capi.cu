@@ -224,6 +224,7 @@ void default_tuning(abf_index* ix) {
     t.probe_cap = 32;
     t.probe_min_fraction = 0.5f;
     t.group_min_queries = 32;
+    t.fixed_tile_shape = 0;
 }
 
 void free_device(abf_index* ix) {
@@ -473,7 +474,18 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
     ta.q_off = b->d_offsets;
     ta.heavy_min = ws->heavy;
     ta.n_q = b->n_queries;
-    ta.n_tiles = uint32_t((n_words + t.tile_words - 1) / t.tile_words);
+    // a batch too small to fill the GPU at the tuned tile shape (the tuner
+    // sees large batches) gets full 8-warp CTAs first, then narrower tiles
+    abf_tuning tt = t;
+    if (!t.fixed_tile_shape) {
+        const uint64_t want = 4ull * uint64_t(ix->sm_count) * 256u;  // threads
+        auto threads = [&]() {
+            return uint64_t(b->n_queries) * ((n_words + tt.tile_words - 1) / tt.tile_words) * tt.warps_per_tile * 32u;
+        };
+        while (tt.warps_per_tile < 8 && threads() < want) tt.warps_per_tile *= 2;
+        while (tt.tile_words > 1024 && threads() < want) tt.tile_words >>= 1;
+    }
+    ta.n_tiles = uint32_t((n_words + tt.tile_words - 1) / tt.tile_words);
     ta.out = b->d_bitmaps;
     ta.out_stride = b->bitmap_stride_words;
     ta.n_words = n_words;
@@ -516,7 +528,7 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
         ga.err = ws->err;
         TIMED(K_GROUP, abf::launch_dense_group(ix->dense_tmap, ga, ix->sm_count, s));
     }
-    TIMED(K_TILE, abf::launch_tile_union(v, ta, t, ix->sm_count, s));
+    TIMED(K_TILE, abf::launch_tile_union(v, ta, tt, ix->sm_count, s));
     abf::ScatterArgs sa{};
     sa.terms = b->d_terms;
     sa.q_off = b->d_offsets;

@@ -22,15 +22,24 @@ from .index import Index
 
 
 def _autotune_union(ix, cfg, lens, sub_batch, device):
-    """The kernels' tuning for this index (dense threshold, tile width, dense
-    group kernel, ...) from the autotuner on 1,024 seeded queries of the
-    config's shape, timed on the list-union path."""
+    """The kernels' tuning for this index from the autotuner on 1,024 seeded
+    queries of the config's shape: the dense threshold and the dense group
+    kernel timed on the list-union path, then the merge kernel's tile shape
+    timed on the hybrid path with its merge threshold (n_ads / 1024) fixed,
+    as the two paths use different kernels."""
     from . import autotune as AT
     q = W.QueriesSpec(1024, cfg.queries.kind, cfg.queries.median, cfg.queries.sigma, cfg.queries.lo,
                       cfg.queries.hi, seed=cfg.queries.seed + 104729)
     qoff, qt = W.gen_queries(q, lens)
-    tr = AT.autotune(ix, qoff, qt, path=N.PATH_UNION, sub_batch=min(sub_batch, 1024), sample=1024, device=device)
-    return dict(tr.best)
+    sb = min(sub_batch, 1024)
+    tu = AT.autotune(ix, qoff, qt, path=N.PATH_UNION, sub_batch=sb, sample=1024, device=device)
+    hm = max(128, cfg.lists.n_ads // 1024)
+    ix.set_tuning(heavy_min_len=hm)
+    knobs = {k: AT.KNOBS[k] for k in ("tile_words", "warps_per_tile", "ctas_per_sm")}
+    knobs["heavy_min_len"] = [hm]
+    th = AT.autotune(ix, qoff, qt, path=N.PATH_HYBRID, sub_batch=sb, sample=1024, knobs=knobs, grid=False,
+                     device=device)
+    return {"union": dict(tu.best), "hybrid_tile_shape": dict(th.best)}
 
 
 def _chunked_features(ix, qoff, qt, chunk, device):

@@ -191,8 +191,10 @@ def test_tuning_sweep_identical(small, tile_words, warps):
     t0 = ix.tuning
     saved = {f: getattr(t0, f) for f, _ in t0._fields_}
     try:
+        # fixed_tile_shape: single queries would otherwise run on adapted
+        # (narrower, 8-warp) tiles, and this sweep is about every shape
         ix.set_tuning(tile_words=tile_words, warps_per_tile=warps, heavy_min_len=64, scatter_blocks_per_warp=3,
-                      probe_chunk_blocks=128)
+                      probe_chunk_blocks=128, fixed_tile_shape=1)
         bm = torch.empty(n_words, dtype=torch.int32, device="cuda")
         for q in small["qs"][::5]:
             for path in (ab.PATH_TILE, ab.PATH_HYBRID, ab.PATH_PROBE):
