@@ -140,6 +140,12 @@ def test_tuning_validation():
             ix.set_tuning(**bad)
     ix.set_tuning(tile_words=512, warps_per_tile=2)
     assert ix.tuning.tile_words == 512 and ix.tuning.warps_per_tile == 2
+    # the fields after probe_min_fraction survive a round trip through the C struct
+    assert ix.tuning.group_min_queries == 32 and ix.tuning.fixed_tile_shape == 0
+    ix.set_tuning(group_min_queries=0, fixed_tile_shape=1, probe_min_fraction=0.25)
+    t = ix.tuning
+    assert t.group_min_queries == 0 and t.fixed_tile_shape == 1 and abs(t.probe_min_fraction - 0.25) < 1e-7
+    assert t.tile_words == 512 and t.warps_per_tile == 2
 
 
 def test_save_load_roundtrip(tmp_path):
