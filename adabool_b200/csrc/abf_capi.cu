@@ -496,15 +496,25 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
     ta.q_ndense = ws->q_ndense;
     ta.q_dmode = ws->q_dmode;
     // dense group kernel: every dense-only query's tiles in one pass per
-    // 32-word tile, when the batch is large enough and the dense bitmaps
-    // (plus the zero row) fit three TMA boxes of 256
+    // tile, when the batch is large enough and the dense bitmaps (plus the
+    // zero row) fit three TMA boxes of 256. Tiles of 64 words (two per lane:
+    // half the index work per word) where two such stages and the batch's
+    // lists (room for 64 per query) fit shared memory and the output rows
+    // are 8-byte aligned, else 32 words.
     const uint32_t n_dense = v.n_dense;
     bool group = t.group_min_queries && b->n_queries >= t.group_min_queries && n_dense > 0 &&
                  n_dense + 1 <= abf::kGroupMaxBoxes * abf::kGroupBoxRows;
-    if (group && (ix->dense_tmap_base != ix->dev.dense || ix->dense_tmap_rows != n_dense)) {
-        if (abf::encode_dense_tmap(v, ix->dense_tmap) == cudaSuccess) {
+    const uint32_t wq = std::min<uint32_t>(b->n_queries, abf::kGroupMaxQueries);
+    const uint32_t gw = (reinterpret_cast<uintptr_t>(b->d_bitmaps) % 8 == 0 && b->bitmap_stride_words % 2 == 0 &&
+                         abf::dense_group_list_cap(n_dense + 1, wq, 64) >= 64u * wq)
+                            ? 64u
+                            : 32u;
+    if (group && (ix->dense_tmap_base != ix->dev.dense || ix->dense_tmap_rows != n_dense ||
+                  ix->dense_tmap_gw != gw)) {
+        if (abf::encode_dense_tmap(v, gw, ix->dense_tmap) == cudaSuccess) {
             ix->dense_tmap_base = ix->dev.dense;
             ix->dense_tmap_rows = n_dense;
+            ix->dense_tmap_gw = gw;
         } else {
             group = false;
         }
@@ -520,13 +530,13 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
         ga.q_dmode = ws->q_dmode + q0;
         ga.n_q = std::min<uint32_t>(abf::kGroupMaxQueries, b->n_queries - q0);
         ga.n_rows = n_dense + 1;
-        ga.list_cap = abf::dense_group_list_cap(ga.n_rows, ga.n_q);
-        ga.n_tiles = uint32_t((n_words + abf::kGroupTileWords - 1) / abf::kGroupTileWords);
+        ga.list_cap = abf::dense_group_list_cap(ga.n_rows, ga.n_q, gw);
+        ga.n_tiles = uint32_t((n_words + gw - 1) / gw);
         ga.out = b->d_bitmaps + uint64_t(q0) * b->bitmap_stride_words;
         ga.out_stride = b->bitmap_stride_words;
         ga.n_words = n_words;
         ga.err = ws->err;
-        TIMED(K_GROUP, abf::launch_dense_group(ix->dense_tmap, ga, ix->sm_count, s));
+        TIMED(K_GROUP, abf::launch_dense_group(ix->dense_tmap, gw, ga, ix->sm_count, s));
     }
     TIMED(K_TILE, abf::launch_tile_union(v, ta, tt, ix->sm_count, s));
     abf::ScatterArgs sa{};

@@ -160,11 +160,12 @@ struct abf_index {
     void* h_stage = nullptr;          // pinned staging for abf_query terms
     size_t h_stage_bytes = 0;
     void* stage_event = nullptr;      // cudaEvent_t guarding the staging buffer
-    // TMA descriptor of the dense bitmaps (2-D: words x bitmaps), encoded on
-    // first use and again when the dense bitmaps change
+    // TMA descriptors of the dense bitmaps (2-D: words x bitmaps), encoded
+    // on first use and again when the dense bitmaps or the tile width change
     alignas(64) unsigned char dense_tmap[256] = {};
     const void* dense_tmap_base = nullptr;
     uint32_t dense_tmap_rows = 0;
+    uint32_t dense_tmap_gw = 0;       // tile words of the boxes (32 or 64)
 };
 
 namespace abf {

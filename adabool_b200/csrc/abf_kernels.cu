@@ -641,61 +641,78 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
 
 constexpr uint32_t kGroupThreads = 1024;
 
-// OR of the 8 rows named by the 16-bit indices in v, column `lane`
-__device__ __forceinline__ uint32_t or8(const uint32_t* S, uint4 v, uint32_t lane) {
-    return S[(v.x & 0xffffu) * kGroupTileWords + lane] | S[(v.x >> 16) * kGroupTileWords + lane] |
-           S[(v.y & 0xffffu) * kGroupTileWords + lane] | S[(v.y >> 16) * kGroupTileWords + lane] |
-           S[(v.z & 0xffffu) * kGroupTileWords + lane] | S[(v.z >> 16) * kGroupTileWords + lane] |
-           S[(v.w & 0xffffu) * kGroupTileWords + lane] | S[(v.w >> 16) * kGroupTileWords + lane];
-}
+// What one lane ORs per row: one word of a 32-word tile, two of a 64-word one.
+template <uint32_t GW> struct GroupWord;
+template <> struct GroupWord<32> { typedef uint32_t T; };
+template <> struct GroupWord<64> { typedef uint2 T; };
+__device__ __forceinline__ uint32_t orw(uint32_t a, uint32_t b) { return a | b; }
+__device__ __forceinline__ uint2 orw(uint2 a, uint2 b) { return make_uint2(a.x | b.x, a.y | b.y); }
+template <typename T> __device__ __forceinline__ T zero_word();
+template <> __device__ __forceinline__ uint32_t zero_word<uint32_t>() { return 0u; }
+template <> __device__ __forceinline__ uint2 zero_word<uint2>() { return make_uint2(0u, 0u); }
 
-// OR over a query's list of nd row indices (padded to a multiple of 8 with
-// the zero row), read 16 at a time from shared or global memory
-__device__ __forceinline__ uint32_t or_list(const uint32_t* S, const uint4* dl, uint32_t nd, uint32_t lane) {
-    uint32_t acc = 0, k = 0;
-    for (; k + 16u <= nd; k += 16u) {
-        const uint4 v0 = dl[k >> 3], v1 = dl[(k >> 3) + 1];
-        acc |= or8(S, v0, lane) | or8(S, v1, lane);
-    }
-    if (k < nd) acc |= or8(S, dl[k >> 3], lane);
-    if (k + 8u < nd) acc |= or8(S, dl[(k >> 3) + 1], lane);
+// Row `woff` (a word offset, row * GW) of a stage, at this lane's column
+// (B = stage + lane * GW / 32 words)
+template <typename T>
+__device__ __forceinline__ T ld_row(const uint8_t* B, uint32_t woff) {
+    return *reinterpret_cast<const T*>(B + (woff << 2));
+}
+// OR of the 8 rows named by the 16-bit word offsets in v
+template <typename T>
+__device__ __forceinline__ T or8w(const uint8_t* B, uint4 v) {
+    return orw(orw(orw(ld_row<T>(B, v.x & 0xffffu), ld_row<T>(B, v.x >> 16)),
+                   orw(ld_row<T>(B, v.y & 0xffffu), ld_row<T>(B, v.y >> 16))),
+               orw(orw(ld_row<T>(B, v.z & 0xffffu), ld_row<T>(B, v.z >> 16)),
+                   orw(ld_row<T>(B, v.w & 0xffffu), ld_row<T>(B, v.w >> 16))));
+}
+// OR over a list of nd word offsets (padded to a multiple of 8 with the
+// zero row), 16 at a time: per row one extract, one address, one shared load
+template <typename T>
+__device__ __forceinline__ T or_list_words(const uint8_t* B, const uint4* ol, uint32_t nd) {
+    T acc = zero_word<T>();
+    uint32_t k = 0;
+    for (; k + 16u <= nd; k += 16u) acc = orw(acc, orw(or8w<T>(B, ol[k >> 3]), or8w<T>(B, ol[(k >> 3) + 1])));
+    if (k < nd) acc = orw(acc, or8w<T>(B, ol[k >> 3]));
+    if (k + 8u < nd) acc = orw(acc, or8w<T>(B, ol[(k >> 3) + 1]));
     return acc;
 }
-
-// OR over a list staged in shared memory as 16-bit word offsets of rows
-// (row * 32), 8 per 16-byte load: per row one extract, one address, one
-// shared load and half a 3-input OR
-__device__ __forceinline__ uint32_t ld_row(const uint8_t* B, uint32_t woff) {
-    return *reinterpret_cast<const uint32_t*>(B + (woff << 2));
-}
-__device__ __forceinline__ uint32_t or8w(const uint8_t* B, uint4 v) {
-    return (ld_row(B, v.x & 0xffffu) | ld_row(B, v.x >> 16) | ld_row(B, v.y & 0xffffu)) |
-           (ld_row(B, v.y >> 16) | ld_row(B, v.z & 0xffffu) | ld_row(B, v.z >> 16)) |
-           (ld_row(B, v.w & 0xffffu) | ld_row(B, v.w >> 16));
-}
-__device__ __forceinline__ uint32_t or_list_words(const uint8_t* B, const uint4* ol, uint32_t nd) {
-    uint32_t acc = 0, k = 0;
-    for (; k + 16u <= nd; k += 16u) acc |= or8w(B, ol[k >> 3]) | or8w(B, ol[(k >> 3) + 1]);
-    if (k < nd) acc |= or8w(B, ol[k >> 3]);
-    if (k + 8u < nd) acc |= or8w(B, ol[(k >> 3) + 1]);
+// the same over a list of 16-bit row indices read from global memory (used
+// when the batch's lists do not fit in shared memory)
+template <uint32_t GW, typename T>
+__device__ __forceinline__ T or_list_rows(const uint8_t* B, const uint4* dl, uint32_t nd) {
+    T acc = zero_word<T>();
+    for (uint32_t k = 0; k < nd; k += 8u) {
+        const uint4 v = dl[k >> 3];
+        const uint4 wv = make_uint4((v.x & 0xffffu) * GW | ((v.x >> 16) * GW) << 16,
+                                    (v.y & 0xffffu) * GW | ((v.y >> 16) * GW) << 16,
+                                    (v.z & 0xffffu) * GW | ((v.z >> 16) * GW) << 16,
+                                    (v.w & 0xffffu) * GW | ((v.w >> 16) * GW) << 16);
+        acc = orw(acc, or8w<T>(B, wv));
+    }
     return acc;
 }
 
 // Shared memory (dynamic, 1024-byte aligned base): two stages of n_rows x
-// 32 words (rows = dense bitmaps + the zero row), then per dense-only query
+// GW words (rows = dense bitmaps + the zero row), then per dense-only query
 // its list's offset and length, the queue of dense-only queries, and the
-// lists themselves as 16-bit row word offsets when they fit (else the
-// 16-bit row lists are read from global memory).
+// lists themselves as 16-bit row word offsets (row * GW) when they fit (else
+// the 16-bit row lists are read from global memory). GW = 64 halves the
+// index work per word (each lane ORs two words per row) where two stages of
+// 64-word rows fit.
+template <uint32_t GW>
 __global__ void __launch_bounds__(kGroupThreads, 1)
     dense_group_kernel(const __grid_constant__ CUtensorMap tmap_full, const __grid_constant__ CUtensorMap tmap_last,
                        DenseGroupArgs a) {
+    typedef typename GroupWord<GW>::T T;
+    constexpr uint32_t kLaneWords = GW / 32u;
+    static_assert(kGroupMaxBoxes * kGroupBoxRows * GW < 65536u, "16-bit word offsets");
     extern __shared__ uint8_t g_raw[];
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ uint32_t s_next[2];
     __shared__ uint32_t s_fail, s_ndq;
     __shared__ uint32_t s_warp[32];
     uint8_t* base = g_raw + ((1024u - (smem_addr(g_raw) & 1023u)) & 1023u);
-    const uint32_t stage_bytes = (a.n_rows * kGroupTileWords * 4u + 1023u) & ~1023u;
+    const uint32_t stage_bytes = (a.n_rows * GW * 4u + 1023u) & ~1023u;
     uint32_t* stage0 = reinterpret_cast<uint32_t*>(base);
     uint32_t* s_meta = reinterpret_cast<uint32_t*>(base + 2u * stage_bytes);  // n_q: list offset / 8 << 16 | nd
     uint16_t* s_qlist = reinterpret_cast<uint16_t*>(s_meta + a.n_q);          // dense-only queries
@@ -707,13 +724,12 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
     const uint32_t full_boxes = (a.n_rows - 1u) / kGroupBoxRows;  // boxes of 256 rows before the last
     auto issue = [&](uint32_t tile, uint32_t st) {  // thread 0 only
         fence_proxy_async();  // earlier reads of this stage (ordered by the barrier) before the copy
-        mbar_expect_tx(&bar[st], a.n_rows * kGroupTileWords * 4u);
+        mbar_expect_tx(&bar[st], a.n_rows * GW * 4u);
         uint32_t* dst = stage0 + st * (stage_bytes / 4u);
         for (uint32_t j = 0; j < full_boxes; ++j)
-            tma_load_2d(dst + j * kGroupBoxRows * kGroupTileWords, &tmap_full, int(tile * kGroupTileWords),
-                        int(j * kGroupBoxRows), &bar[st]);
-        tma_load_2d(dst + full_boxes * kGroupBoxRows * kGroupTileWords, &tmap_last, int(tile * kGroupTileWords),
-                    int(full_boxes * kGroupBoxRows), &bar[st]);
+            tma_load_2d(dst + j * kGroupBoxRows * GW, &tmap_full, int(tile * GW), int(j * kGroupBoxRows), &bar[st]);
+        tma_load_2d(dst + full_boxes * kGroupBoxRows * GW, &tmap_last, int(tile * GW), int(full_boxes * kGroupBoxRows),
+                    &bar[st]);
     };
     if (tid == 0) {
         mbar_init(&bar[0], 1);
@@ -751,16 +767,15 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
     if (tid == 0) s_ndq = tot_cnt;
     __syncthreads();
     if (in_smem) {
+        constexpr uint32_t kShift = GW == 64u ? 6u : 5u;  // row -> word offset, both halves at once
         for (uint32_t i = warp; i < tot_cnt; i += kNW) {  // a warp per query, 16 bytes per lane
             const uint32_t q = s_qlist[i];
             const uint32_t m = s_meta[q];
             const uint4* src = reinterpret_cast<const uint4*>(a.q_dense16 + a.q_dstart[q]);
             uint4* dst = s_lists + (m >> 16);
-            // rows -> word offsets (row * 32 < 2^15: both halves shift together)
-            static_assert(kGroupTileWords == 32u && kGroupMaxBoxes * kGroupBoxRows * 32u < 65536u, "offsets");
             for (uint32_t j = lane; j < ((m & 0xffffu) + 7u) / 8u; j += 32u) {
                 const uint4 v = src[j];
-                dst[j] = make_uint4(v.x << 5, v.y << 5, v.z << 5, v.w << 5);
+                dst[j] = make_uint4(v.x << kShift, v.y << kShift, v.z << kShift, v.w << kShift);
             }
         }
     }
@@ -789,8 +804,8 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
             return;
         }
         const uint32_t* S = stage0 + st * (stage_bytes / 4u);
-        const uint8_t* B = reinterpret_cast<const uint8_t*>(S + lane);
-        const uint64_t w = uint64_t(t) * kGroupTileWords + lane;
+        const uint8_t* B = reinterpret_cast<const uint8_t*>(S + lane * kLaneWords);
+        const uint64_t w = uint64_t(t) * GW + lane * kLaneWords;
         for (;;) {
             uint32_t i = 0;
             if (lane == 0) i = atomicAdd(&s_next[st], 1u);
@@ -799,10 +814,16 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
             const uint32_t q = s_qlist[i];
             const uint32_t m = s_meta[q];
             const uint32_t nd = m & 0xffffu;
-            const uint32_t acc =
-                in_smem ? or_list_words(B, s_lists + (m >> 16), nd)
-                        : or_list(S, reinterpret_cast<const uint4*>(a.q_dense16 + a.q_dstart[q]), nd, lane);
-            if (w < a.n_words) a.out[uint64_t(q) * a.out_stride + w] = acc;
+            const T acc = in_smem ? or_list_words<T>(B, s_lists + (m >> 16), nd)
+                                  : or_list_rows<GW, T>(B, reinterpret_cast<const uint4*>(a.q_dense16 + a.q_dstart[q]),
+                                                        nd);
+            uint32_t* o = a.out + uint64_t(q) * a.out_stride + w;
+            if constexpr (GW == 64u) {
+                if (w + 1u < a.n_words) *reinterpret_cast<uint2*>(o) = acc;  // 8-byte aligned (checked at launch)
+                else if (w < a.n_words) o[0] = acc.x;
+            } else {
+                if (w < a.n_words) o[0] = acc;
+            }
         }
         __syncthreads();  // this stage is read; the next iteration may refill it
         if (tid == 0) s_next[st] = 0;
@@ -1366,10 +1387,10 @@ EncodeTiledFn encoder() {
 }
 }  // namespace
 
-cudaError_t encode_dense_tmap(const IndexView& v, void* out) {
+cudaError_t encode_dense_tmap(const IndexView& v, uint32_t gw, void* out) {
     static_assert(sizeof(CUtensorMap) == 128, "tensor map size");
     EncodeTiledFn fn = encoder();
-    if (!fn || !v.dense || v.n_dense == 0) return cudaErrorNotSupported;
+    if (!fn || !v.dense || v.n_dense == 0 || (gw != 32u && gw != 64u)) return cudaErrorNotSupported;
     // dims: words of a bitmap (innermost), bitmaps; rows past n_dense read as
     // zeros. Two descriptors: boxes of 256 bitmaps, and one box for the rest
     // plus the zero row, so a stage holds exactly n_dense + 1 rows.
@@ -1379,7 +1400,7 @@ cudaError_t encode_dense_tmap(const IndexView& v, void* out) {
     const cuuint64_t strides[1] = {cuuint64_t(v.dense_stride) * 4u};
     const cuuint32_t es[2] = {1, 1};
     for (int k = 0; k < 2; ++k) {
-        const cuuint32_t box[2] = {kGroupTileWords, k == 0 ? kGroupBoxRows : last};
+        const cuuint32_t box[2] = {gw, k == 0 ? kGroupBoxRows : last};
         const CUresult r = fn(reinterpret_cast<CUtensorMap*>(out) + k, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2,
                               const_cast<uint32_t*>(v.dense), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
                               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -1389,32 +1410,46 @@ cudaError_t encode_dense_tmap(const IndexView& v, void* out) {
     return cudaSuccess;
 }
 
-uint32_t dense_group_list_cap(uint32_t n_rows, uint32_t n_q) {
-    const uint64_t stage = (uint64_t(n_rows) * kGroupTileWords * 4u + 1023u) & ~1023ull;
+uint32_t dense_group_list_cap(uint32_t n_rows, uint32_t n_q, uint32_t gw) {
+    const uint64_t stage = (uint64_t(n_rows) * gw * 4u + 1023u) & ~1023ull;
     const uint64_t used = 1024u + 2u * stage + ((6ull * n_q + 15u) & ~15ull);
     return used >= kGroupSmemBytes ? 0u : uint32_t((kGroupSmemBytes - used) / 2u) & ~7u;
 }
 
-cudaError_t launch_dense_group(const void* tmaps, const DenseGroupArgs& a, int sm_count, cudaStream_t s) {
-    if (a.n_q == 0 || a.n_tiles == 0) return cudaSuccess;
-    if (a.n_rows < 2 || a.n_rows > kGroupMaxBoxes * kGroupBoxRows || a.n_q > kGroupMaxQueries)
-        return cudaErrorInvalidValue;
+namespace {
+template <uint32_t GW>
+cudaError_t launch_group_w(const CUtensorMap (&m)[2], const DenseGroupArgs& a, int sm_count, cudaStream_t s) {
     static std::atomic<uint64_t> done{0};  // devices whose attribute is set
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (!(done.load() >> dev & 1ull)) {
-        e = cudaFuncSetAttribute(dense_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(dense_group_kernel<GW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(kGroupSmemBytes));
         if (e != cudaSuccess) return e;
         done.fetch_or(1ull << dev);
     }
+    const uint32_t grid = a.n_tiles < uint32_t(sm_count) ? a.n_tiles : uint32_t(sm_count);
+    dense_group_kernel<GW><<<grid, kGroupThreads, kGroupSmemBytes, s>>>(m[0], m[1], a);
+    return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_dense_group(const void* tmaps, uint32_t gw, const DenseGroupArgs& a, int sm_count,
+                               cudaStream_t s) {
+    if (a.n_q == 0 || a.n_tiles == 0) return cudaSuccess;
+    if (a.n_rows < 2 || a.n_rows > kGroupMaxBoxes * kGroupBoxRows || a.n_q > kGroupMaxQueries)
+        return cudaErrorInvalidValue;
+    const uint64_t stage = (uint64_t(a.n_rows) * gw * 4u + 1023u) & ~1023ull;
+    if (1024u + 2u * stage + ((6ull * a.n_q + 15u) & ~15ull) > kGroupSmemBytes) return cudaErrorInvalidValue;
     CUtensorMap m[2];
     std::memcpy(m, tmaps, sizeof(m));
-    const uint32_t grid = a.n_tiles < uint32_t(sm_count) ? a.n_tiles : uint32_t(sm_count);
-    dense_group_kernel<<<grid, kGroupThreads, kGroupSmemBytes, s>>>(m[0], m[1], a);
+    cudaError_t e;
+    if (gw == 64u) e = launch_group_w<64>(m, a, sm_count, s);
+    else if (gw == 32u) e = launch_group_w<32>(m, a, sm_count, s);
+    else return cudaErrorInvalidValue;
     count_launch();
-    return cudaGetLastError();
+    return e;
 }
 
 cudaError_t launch_scatter(const IndexView& v, const ScatterArgs& a, const abf_tuning& t, int sm_count,

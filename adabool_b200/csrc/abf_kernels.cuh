@@ -108,8 +108,7 @@ struct TileArgs {
     int skip_dense_only;
 };
 
-// dense group kernel: one pass per 32-word tile over all dense-only queries
-constexpr uint32_t kGroupTileWords = 32;
+// dense group kernel: one pass per 32- or 64-word tile over all dense-only queries
 constexpr uint32_t kGroupBoxRows = 256;   // dense bitmaps per TMA box
 constexpr uint32_t kGroupMaxBoxes = 3;    // up to 767 dense bitmaps plus the zero row
 constexpr uint32_t kGroupMaxQueries = 2048;
@@ -123,7 +122,7 @@ struct DenseGroupArgs {
     uint32_t n_q;              // <= kGroupMaxQueries
     uint32_t n_rows;           // n_dense + 1 (the last row reads as zeros)
     uint32_t list_cap;         // list entries (16-bit row word offsets) that fit in shared memory
-    uint32_t n_tiles;          // ceil(n_words / 32)
+    uint32_t n_tiles;          // ceil(n_words / tile words)
     uint32_t* out;
     uint64_t out_stride;
     uint64_t n_words;
@@ -179,12 +178,15 @@ uint64_t scan_tiles(uint64_t n);
 
 cudaError_t launch_plan(const IndexView& v, const PlanArgs& a, cudaStream_t s);
 // two 2-D TMA descriptors (2 x 128 bytes into out) of the dense bitmaps:
-// 32-word x 256-bitmap boxes, and one box for the remaining bitmaps plus the
-// zero row; cudaErrorNotSupported when the driver has no encoder
-cudaError_t encode_dense_tmap(const IndexView& v, void* out);
-// list entries (16-bit row word offsets) the group kernel can stage in shared memory
-uint32_t dense_group_list_cap(uint32_t n_rows, uint32_t n_q);
-cudaError_t launch_dense_group(const void* tmaps, const DenseGroupArgs& a, int sm_count, cudaStream_t s);
+// gw-word (32 or 64) x 256-bitmap boxes, and one box for the remaining
+// bitmaps plus the zero row; cudaErrorNotSupported when the driver has no
+// encoder
+cudaError_t encode_dense_tmap(const IndexView& v, uint32_t gw, void* out);
+// list entries (16-bit row word offsets) the group kernel can stage in shared
+// memory with gw-word tiles (0: two stages do not fit)
+uint32_t dense_group_list_cap(uint32_t n_rows, uint32_t n_q, uint32_t gw);
+cudaError_t launch_dense_group(const void* tmaps, uint32_t gw, const DenseGroupArgs& a, int sm_count,
+                               cudaStream_t s);
 cudaError_t launch_queue_scan(const QueueArgs& a, cudaStream_t s);
 cudaError_t launch_probe_bits(const ProbeBitsArgs& a, uint32_t probe_cap, cudaStream_t s);
 cudaError_t launch_tile_union(const IndexView& v, const TileArgs& a, const abf_tuning& t, int sm_count,
