@@ -505,10 +505,14 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
     bool group = t.group_min_queries && b->n_queries >= t.group_min_queries && n_dense > 0 &&
                  n_dense + 1 <= abf::kGroupMaxBoxes * abf::kGroupBoxRows;
     const uint32_t wq = std::min<uint32_t>(b->n_queries, abf::kGroupMaxQueries);
-    const uint32_t gw = (reinterpret_cast<uintptr_t>(b->d_bitmaps) % 8 == 0 && b->bitmap_stride_words % 2 == 0 &&
-                         abf::dense_group_list_cap(n_dense + 1, wq, 64) >= 64u * wq)
-                            ? 64u
-                            : 32u;
+    const bool out8 = reinterpret_cast<uintptr_t>(b->d_bitmaps) % 8 == 0 && b->bitmap_stride_words % 2 == 0;
+    uint32_t gw = 32, stages = 2;
+    if (out8 && abf::dense_group_list_cap(n_dense + 1, wq, 64, 2) >= 64u * wq) {
+        gw = 64;
+    } else if (out8 && abf::dense_group_list_cap(n_dense + 1, wq, 64, 1) >= 64u * wq) {
+        gw = 64;
+        stages = 1;
+    }
     if (group && (ix->dense_tmap_base != ix->dev.dense || ix->dense_tmap_rows != n_dense ||
                   ix->dense_tmap_gw != gw)) {
         if (abf::encode_dense_tmap(v, gw, ix->dense_tmap) == cudaSuccess) {
@@ -530,7 +534,8 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
         ga.q_dmode = ws->q_dmode + q0;
         ga.n_q = std::min<uint32_t>(abf::kGroupMaxQueries, b->n_queries - q0);
         ga.n_rows = n_dense + 1;
-        ga.list_cap = abf::dense_group_list_cap(ga.n_rows, ga.n_q, gw);
+        ga.stages = stages;
+        ga.list_cap = abf::dense_group_list_cap(ga.n_rows, ga.n_q, gw, stages);
         ga.n_tiles = uint32_t((n_words + gw - 1) / gw);
         ga.out = b->d_bitmaps + uint64_t(q0) * b->bitmap_stride_words;
         ga.out_stride = b->bitmap_stride_words;

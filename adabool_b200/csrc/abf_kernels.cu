@@ -713,10 +713,11 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
     __shared__ uint32_t s_warp[32];
     uint8_t* base = g_raw + ((1024u - (smem_addr(g_raw) & 1023u)) & 1023u);
     const uint32_t stage_bytes = (a.n_rows * GW * 4u + 1023u) & ~1023u;
+    const bool dbl = a.stages == 2u;  // two stages: the next tile's copy overlaps this tile's merge
     uint32_t* stage0 = reinterpret_cast<uint32_t*>(base);
-    uint32_t* s_meta = reinterpret_cast<uint32_t*>(base + 2u * stage_bytes);  // n_q: list offset / 8 << 16 | nd
-    uint16_t* s_qlist = reinterpret_cast<uint16_t*>(s_meta + a.n_q);          // dense-only queries
-    uint4* s_lists = reinterpret_cast<uint4*>(base + 2u * stage_bytes + ((6u * a.n_q + 15u) & ~15u));  // 8 offsets each
+    uint32_t* s_meta = reinterpret_cast<uint32_t*>(base + a.stages * stage_bytes);  // n_q: list offset / 8 << 16 | nd
+    uint16_t* s_qlist = reinterpret_cast<uint16_t*>(s_meta + a.n_q);               // dense-only queries
+    uint4* s_lists = reinterpret_cast<uint4*>(base + a.stages * stage_bytes + ((6u * a.n_q + 15u) & ~15u));
     const uint32_t tid = threadIdx.x, lane = lane_id(), warp = warp_id();
     constexpr uint32_t kNW = kGroupThreads / 32u;
     uint32_t t = blockIdx.x;
@@ -783,9 +784,9 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
     const uint32_t n_dq = s_ndq;
     uint32_t phase = 0;  // bit s: parity of stage s's next completion
     for (uint32_t it = 0; t < a.n_tiles; ++it, t += gridDim.x) {
-        const uint32_t st = it & 1u;
+        const uint32_t st = dbl ? (it & 1u) : 0u;
         const bool more = t + gridDim.x < a.n_tiles;
-        if (tid == 0 && more) issue(t + gridDim.x, st ^ 1u);
+        if (tid == 0 && more && dbl) issue(t + gridDim.x, st ^ 1u);
         uint32_t spins = 0;
         while (!mbar_try_wait(&bar[st], (phase >> st) & 1u)) {
             if (++spins > kSpinLimit) {
@@ -796,7 +797,7 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
         phase ^= 1u << st;
         if (__syncthreads_or(s_fail)) {
             if (tid == 0) atomicOr(a.err, kErrTmaTimeout);
-            if (more) {  // let the other stage's copy land before the CTA leaves
+            if (more && dbl) {  // let the other stage's copy land before the CTA leaves
                 uint32_t sp = 0;
                 while (!mbar_try_wait(&bar[st ^ 1u], (phase >> (st ^ 1u)) & 1u) && ++sp < kSpinLimit) {
                 }
@@ -826,7 +827,12 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
             }
         }
         __syncthreads();  // this stage is read; the next iteration may refill it
-        if (tid == 0) s_next[st] = 0;
+        if (tid == 0) {
+            s_next[st] = 0;
+            // one stage: the next tile's copy starts now that every warp is
+            // done with this one (the arrive in issue() publishes the reset)
+            if (!dbl && more) issue(t + gridDim.x, 0u);
+        }
     }
 }
 
@@ -1410,9 +1416,9 @@ cudaError_t encode_dense_tmap(const IndexView& v, uint32_t gw, void* out) {
     return cudaSuccess;
 }
 
-uint32_t dense_group_list_cap(uint32_t n_rows, uint32_t n_q, uint32_t gw) {
+uint32_t dense_group_list_cap(uint32_t n_rows, uint32_t n_q, uint32_t gw, uint32_t stages) {
     const uint64_t stage = (uint64_t(n_rows) * gw * 4u + 1023u) & ~1023ull;
-    const uint64_t used = 1024u + 2u * stage + ((6ull * n_q + 15u) & ~15ull);
+    const uint64_t used = 1024u + stages * stage + ((6ull * n_q + 15u) & ~15ull);
     return used >= kGroupSmemBytes ? 0u : uint32_t((kGroupSmemBytes - used) / 2u) & ~7u;
 }
 
@@ -1441,7 +1447,9 @@ cudaError_t launch_dense_group(const void* tmaps, uint32_t gw, const DenseGroupA
     if (a.n_rows < 2 || a.n_rows > kGroupMaxBoxes * kGroupBoxRows || a.n_q > kGroupMaxQueries)
         return cudaErrorInvalidValue;
     const uint64_t stage = (uint64_t(a.n_rows) * gw * 4u + 1023u) & ~1023ull;
-    if (1024u + 2u * stage + ((6ull * a.n_q + 15u) & ~15ull) > kGroupSmemBytes) return cudaErrorInvalidValue;
+    if ((a.stages != 1u && a.stages != 2u) ||
+        1024u + a.stages * stage + ((6ull * a.n_q + 15u) & ~15ull) > kGroupSmemBytes)
+        return cudaErrorInvalidValue;
     CUtensorMap m[2];
     std::memcpy(m, tmaps, sizeof(m));
     cudaError_t e;

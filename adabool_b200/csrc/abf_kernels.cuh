@@ -122,6 +122,7 @@ struct DenseGroupArgs {
     uint32_t n_q;              // <= kGroupMaxQueries
     uint32_t n_rows;           // n_dense + 1 (the last row reads as zeros)
     uint32_t list_cap;         // list entries (16-bit row word offsets) that fit in shared memory
+    uint32_t stages;           // 2: double-buffered tile copies; 1: one stage, refilled after each tile
     uint32_t n_tiles;          // ceil(n_words / tile words)
     uint32_t* out;
     uint64_t out_stride;
@@ -183,8 +184,8 @@ cudaError_t launch_plan(const IndexView& v, const PlanArgs& a, cudaStream_t s);
 // encoder
 cudaError_t encode_dense_tmap(const IndexView& v, uint32_t gw, void* out);
 // list entries (16-bit row word offsets) the group kernel can stage in shared
-// memory with gw-word tiles (0: two stages do not fit)
-uint32_t dense_group_list_cap(uint32_t n_rows, uint32_t n_q, uint32_t gw);
+// memory with gw-word tiles and `stages` stages (0: the stages do not fit)
+uint32_t dense_group_list_cap(uint32_t n_rows, uint32_t n_q, uint32_t gw, uint32_t stages);
 cudaError_t launch_dense_group(const void* tmaps, uint32_t gw, const DenseGroupArgs& a, int sm_count,
                                cudaStream_t s);
 cudaError_t launch_queue_scan(const QueueArgs& a, cudaStream_t s);

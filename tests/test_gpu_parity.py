@@ -112,12 +112,13 @@ def test_batch_mixed_paths_and_probe_overflow(small):
         ix.set_tuning(probe_cap=old)
 
 
-@pytest.mark.parametrize("dense_div", [16, 128, 512, 4096])
+@pytest.mark.parametrize("dense_div", [16, 128, 512, 1024, 4096])
 @pytest.mark.parametrize("path", [ab.PATH_UNION, ab.PATH_HYBRID, ab.PATH_AUTO, "mixed"])
 def test_dense_group_kernel(small, dense_div, path):
-    """The dense group kernel (one pass per 32-word tile over every
-    dense-only query, dense slices staged by TMA) against the oracle, on and
-    off, with 1, 2 or 3 TMA boxes of dense bitmaps or too many for it."""
+    """The dense group kernel (one pass per tile over every dense-only query,
+    dense slices staged by TMA) against the oracle, on and off, with 1, 2 or
+    3 TMA boxes of dense bitmaps (12 / 83 / 295 / 553 of them: 64-word tiles
+    double-buffered, then single-buffered) or too many for it (1,914)."""
     torch = _torch()
     ix, n_words, qs = small["ix"], small["n_words"], small["qs"]
     old_dd, old_gm = ix.dense_div, ix.tuning.group_min_queries
