@@ -152,9 +152,10 @@ typedef struct abf_tuning {
                                  of all blocks, else list-union */
     uint32_t group_min_queries; /* batches of at least this many queries merge the
                                  dense bitmaps of all their dense-only queries in one
-                                 pass per 32-word tile (each tile's slice of every dense
-                                 bitmap staged once in shared memory by TMA, then ORed
-                                 per query); needs at most 767 dense bitmaps; 0 = never */
+                                 pass per 64- or 32-word tile (each tile's slice of every
+                                 dense bitmap staged once in shared memory by TMA, then
+                                 ORed per query); needs at most 767 dense bitmaps;
+                                 0 = never */
     uint32_t fixed_tile_shape;  /* 0: a batch too small to fill the GPU at tile_words x
                                  warps_per_tile runs the merge kernel with 8-warp CTAs
                                  and tiles narrowed down to 1,024 words; 1: always the
