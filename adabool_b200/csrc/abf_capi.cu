@@ -495,7 +495,7 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
     ta.q_dstart = ws->q_dstart;
     ta.q_ndense = ws->q_ndense;
     ta.q_dmode = ws->q_dmode;
-    // dense group kernel: every dense-only query's tiles in one pass per
+    // dense group kernel: the dense lists of every non-probe query in one pass per
     // tile, when the batch is large enough and the dense bitmaps (plus the
     // zero row) fit three TMA boxes of 256. Tiles of 64 words (two per lane:
     // half the index work per word) where two such stages and the batch's

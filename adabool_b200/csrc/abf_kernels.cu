@@ -337,7 +337,9 @@ __global__ void __launch_bounds__(256) plan_kernel(IndexView ix, PlanArgs a) {
             if (tid == 0) {
                 a.q_dstart[q] = start;
                 a.q_ndense[q] = nd;
-                a.q_dmode[q] = (!probe && qe > qb && !any_merge) ? 1u : 0u;
+                // 1: every list it merges has a dense bitmap; 2: it also merges
+                // lists without one; 0: probe or empty (no dense merge at all)
+                a.q_dmode[q] = (!probe && qe > qb) ? (any_merge ? 2u : 1u) : 0u;
             }
         }
         if (tid == 0) {
@@ -510,7 +512,8 @@ __global__ void __launch_bounds__(NW * 32) tile_union_kernel(IndexView ix, TileA
                 for (uint32_t i = tid; i < nw; i += NT) dst[i] = 0u;
             continue;
         }
-        if (a.q_dense16 && !a.accumulate && a.q_dmode[q]) {
+        const uint32_t dmode = a.q_dense16 ? a.q_dmode[q] : 0u;
+        if (a.q_dense16 && !a.accumulate && dmode == 1u) {
             // every merged list has a dense bitmap: the dense group kernel
             // writes this tile, or each thread ORs its 16-byte slots over the
             // query's dense slices, KT loads in flight, and stores the
@@ -519,7 +522,11 @@ __global__ void __launch_bounds__(NW * 32) tile_union_kernel(IndexView ix, TileA
                 dense_only_tile<W, NT>(ix, a.q_dense16 + a.q_dstart[q], a.q_ndense[q], t, dst, nw, a.vec_ok != 0);
             continue;
         }
-        for (uint32_t i = tid; i < uint32_t(W); i += NT) tile[i] = (a.accumulate && i < nw) ? dst[i] : 0u;
+        // with the dense group kernel on, a query that also merges lists
+        // without dense bitmaps already has its dense lists in the output:
+        // the tile starts from it and adds only the others
+        const bool on_group = a.skip_dense_only && dmode == 2u && !a.accumulate;
+        for (uint32_t i = tid; i < uint32_t(W); i += NT) tile[i] = ((a.accumulate || on_group) && i < nw) ? dst[i] : 0u;
         if (tid == 0) s_ndense = 0;
         __syncthreads();
         for (uint64_t c0 = qb; c0 < qe; c0 += NT) {
@@ -527,8 +534,11 @@ __global__ void __launch_bounds__(NW * 32) tile_union_kernel(IndexView ix, TileA
             uint32_t lo = 0, cnt = 0;
             const uint32_t cls = i < qe ? __ldg(a.tile_cls + i) : kNone;
             if (cls != kNone) {
-                if (cls & kDenseFlag) s_dense[atomicAdd(&s_ndense, 1u)] = cls & ~kDenseFlag;
-                else tile_block_range(ix, cls, lo_id, hi_id, dj0, dj1, lo, cnt);
+                if (cls & kDenseFlag) {
+                    if (!on_group) s_dense[atomicAdd(&s_ndense, 1u)] = cls & ~kDenseFlag;
+                } else {
+                    tile_block_range(ix, cls, lo_id, hi_id, dj0, dj1, lo, cnt);
+                }
             }
             uint32_t total;
             const uint32_t ex = block_excl_scan<NT>(cnt, s_warp, &total);
@@ -623,13 +633,14 @@ __global__ void __launch_bounds__(NW * 32) tile_union_kernel(IndexView ix, TileA
 }
 
 // ---------------------------------------------------------------------------
-// list-union, dense group variant: one CTA per SM walks 32-word tiles; for
-// each tile, a 2-D TMA copy stages that tile's slice of every dense bitmap
-// in shared memory once (double-buffered: the next tile's copy is in flight
-// while this one is merged), then every dense-only query of the batch ORs
-// its dense slices from shared memory and writes its 32 words. Dense bitmaps
-// shared by many queries are read from L2 / HBM once per tile instead of
-// once per query and tile.
+// list-union, dense group variant: one CTA per SM walks 64- or 32-word
+// tiles; for each tile, a 2-D TMA copy stages that tile's slice of every
+// dense bitmap in shared memory once (double-buffered where two stages fit:
+// the next tile's copy is in flight while this one is merged), then every
+// non-probe query of the batch ORs its dense slices from shared memory and
+// writes its tile (the merge kernel later adds the lists without dense
+// bitmaps that a query merges). Dense bitmaps shared by many queries are
+// read from L2 / HBM once per tile instead of once per query and tile.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
     asm volatile(
@@ -693,8 +704,8 @@ __device__ __forceinline__ T or_list_rows(const uint8_t* B, const uint4* dl, uin
 }
 
 // Shared memory (dynamic, 1024-byte aligned base): two stages of n_rows x
-// GW words (rows = dense bitmaps + the zero row), then per dense-only query
-// its list's offset and length, the queue of dense-only queries, and the
+// GW words (rows = dense bitmaps + the zero row), then per such query
+// its list's offset and length, the queue of those queries, and the
 // lists themselves as 16-bit row word offsets (row * GW) when they fit (else
 // the 16-bit row lists are read from global memory). GW = 64 halves the
 // index work per word (each lane ORs two words per row) where two stages of
@@ -716,7 +727,7 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
     const bool dbl = a.stages == 2u;  // two stages: the next tile's copy overlaps this tile's merge
     uint32_t* stage0 = reinterpret_cast<uint32_t*>(base);
     uint32_t* s_meta = reinterpret_cast<uint32_t*>(base + a.stages * stage_bytes);  // n_q: list offset / 8 << 16 | nd
-    uint16_t* s_qlist = reinterpret_cast<uint16_t*>(s_meta + a.n_q);               // dense-only queries
+    uint16_t* s_qlist = reinterpret_cast<uint16_t*>(s_meta + a.n_q);               // queries with q_dmode != 0
     uint4* s_lists = reinterpret_cast<uint4*>(base + a.stages * stage_bytes + ((6u * a.n_q + 15u) & ~15u));
     const uint32_t tid = threadIdx.x, lane = lane_id(), warp = warp_id();
     constexpr uint32_t kNW = kGroupThreads / 32u;
@@ -740,7 +751,7 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
         s_fail = 0;
         issue(t, 0);  // the first tile's copy overlaps the list staging below
     }
-    // stage the dense-only queries' lists (the same for every tile): offsets
+    // stage those queries' lists (the same for every tile): offsets
     // by a block scan over the queries, at most two per thread
     uint32_t len[2], cnt[2];
 #pragma unroll

@@ -64,7 +64,8 @@ struct PlanArgs {
     uint16_t* q_dense16;      // out: max_terms + 8 * n_q + 16 entries
     uint32_t* q_dstart;       // out: per query
     uint32_t* q_ndense;       // out: per query, distinct dense bitmaps
-    uint32_t* q_dmode;        // out: per query, 1 if every list it merges has a dense bitmap
+    uint32_t* q_dmode;        // out: per query, 1 if every list it merges has a dense bitmap,
+                              // 2 if it also merges lists without one, 0 for probe / empty
 };
 
 constexpr uint32_t kDenseFlag = 0x80000000u;
@@ -98,9 +99,11 @@ struct TileArgs {
     int accumulate;           // 1: OR into the existing bitmap, 0: overwrite
     int vec_ok;               // out 16-byte aligned and out_stride % 4 == 0
     // optional (plan kernel): queries whose merged lists all have dense
-    // bitmaps (q_dmode) take a barrier-free path that streams the OR of their
-    // slices straight to the output, or are skipped when the dense group
-    // kernel covers them
+    // bitmaps (q_dmode 1) take a barrier-free path that streams the OR of
+    // their slices straight to the output, or are skipped when the dense
+    // group kernel covers them; with the group kernel on (skip_dense_only),
+    // q_dmode 2 queries start their tiles from its output and merge only
+    // their lists without dense bitmaps
     const uint16_t* q_dense16;
     const uint32_t* q_dstart;
     const uint32_t* q_ndense;
