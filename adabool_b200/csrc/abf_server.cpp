@@ -12,6 +12,7 @@
 // shared state (the waiting queue, the pool, the finished results) sits
 // behind one mutex that is never held across a CUDA call.
 #include "abf_kernels.cuh"
+#include "abf_pool.h"
 
 #include <algorithm>
 #include <atomic>
@@ -41,57 +42,6 @@ uint64_t now_ns() {
 constexpr uint64_t kAlign = 256;
 constexpr uint32_t kMaxStreams = 8;
 uint64_t align_up(uint64_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
-
-// First-fit allocator over one device range. Free extents are kept by
-// offset and merged with their neighbours when a range comes back, so a
-// pool whose results were all released is one extent again.
-class Pool {
-  public:
-    static constexpr uint64_t kFail = ~0ull;
-    void reset(uint64_t size) {
-        free_.clear();
-        if (size) free_[0] = size;
-        used_ = 0;
-    }
-    uint64_t alloc(uint64_t n) {
-        for (auto it = free_.begin(); it != free_.end(); ++it) {
-            if (it->second < n) continue;
-            const uint64_t off = it->first, left = it->second - n;
-            free_.erase(it);
-            if (left) free_[off + n] = left;
-            used_ += n;
-            return off;
-        }
-        return kFail;
-    }
-    void release(uint64_t off, uint64_t n) {
-        if (!n) return;
-        used_ -= n;
-        auto next = free_.lower_bound(off);
-        if (next != free_.end() && off + n == next->first) {
-            n += next->second;
-            next = free_.erase(next);
-        }
-        if (next != free_.begin()) {
-            auto prev = std::prev(next);
-            if (prev->first + prev->second == off) {
-                prev->second += n;
-                return;
-            }
-        }
-        free_[off] = n;
-    }
-    uint64_t largest() const {
-        uint64_t m = 0;
-        for (const auto& e : free_) m = std::max(m, e.second);
-        return m;
-    }
-    uint64_t used() const { return used_; }
-
-  private:
-    std::map<uint64_t, uint64_t> free_;
-    uint64_t used_ = 0;
-};
 
 struct Batch;
 
@@ -142,7 +92,7 @@ struct abf_server {
     uint64_t bm_bytes = 0;  // one query's bitmap
     uint8_t* pool_base = nullptr;
     uint64_t pool_bytes = 0;
-    Pool pool;
+    abf::Pool pool;
     std::vector<Slot> slots;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
