@@ -143,9 +143,12 @@ PROTOTYPES = {
     "abf_batch_list_union_sparse": [vp, vp, vp, C.c_uint32, vp],
     "abf_collect_ids": [vp, vp, C.c_uint64, vp, C.c_uint64, vp, vp],
     "abf_collect_ids_noalloc": [vp, C.c_uint64, vp, C.c_uint64, vp, vp],
+    "abf_collect_ids_noalloc_check": [vp],
     "abf_workspace_create": [vp, C.c_uint32, C.c_uint64, C.POINTER(vp)],
     "abf_workspace_free": [vp],
     "abf_workspace_check": [vp, vp],
+    "abf_workspace_set_wait_limit": [vp, C.c_uint32],
+    "abf_workspace_selftest_waits": [vp, C.c_uint32, vp],
     "abf_batch_run": [vp, vp, C.POINTER(Batch), vp],
     "abf_query": [vp, u32p, C.c_uint32, C.c_int, vp, vp, C.c_uint64, vp, vp],
     "abf_planner_features": [vp, vp, vp, C.c_uint32, vp, vp],

@@ -56,11 +56,9 @@ using abf::fail;
 namespace {
 
 // ---- kernel timing (abf_profile_enable / abf_profile_read) ----
-enum Kid { K_PLAN, K_QUEUE, K_PROBE_BITS, K_TILE, K_SCATTER, K_PROBE, K_COUNT, K_SCAN, K_WRITE, K_PLANNER,
-           K_GROUP, K_NKERNELS };
-const char* const kKernelNames[K_NKERNELS] = {"plan",   "queue_scan",    "probe_bits",   "tile_union",
-                                              "scatter_union", "probe", "compact_count", "compact_scan",
-                                              "compact_write", "planner",    "dense_group"};
+enum Kid { K_PLAN, K_QUEUE, K_PROBE_BITS, K_TILE, K_SCATTER, K_PROBE, K_COMPACT, K_PLANNER, K_GROUP, K_NKERNELS };
+const char* const kKernelNames[K_NKERNELS] = {"plan",  "queue_scan", "probe_bits", "tile_union", "scatter_union",
+                                              "probe", "compact",    "planner",    "dense_group"};
 
 struct Profiler {
     struct Rec {
@@ -133,10 +131,8 @@ struct abf_workspace {
     uint32_t* probe_list = nullptr;
     uint32_t* n_probe = nullptr;
     uint32_t* probe_bm = nullptr;
-    uint32_t* counts = nullptr;
-    uint64_t* offsets = nullptr;
-    uint64_t* scan_status = nullptr;
-    uint32_t* scan_counter = nullptr;
+    uint64_t* scan_status = nullptr;         // compaction look-back words, one per chunk (+1)
+    unsigned long long* ticket = nullptr;   // compaction item counter
     uint64_t* id_off = nullptr;
     uint8_t* path_out = nullptr;
     uint8_t* auto_paths = nullptr;  // planner choices for ABF_PATH_AUTO batches
@@ -145,8 +141,11 @@ struct abf_workspace {
     uint32_t* q_ndense = nullptr;   // per query
     uint32_t* q_dmode = nullptr;    // per query
     uint32_t* err = nullptr;
+    uint32_t* tile_list = nullptr;  // queries the merge kernel visits beside the dense group kernel
+    uint32_t* n_tile_list = nullptr;
     uint32_t* q_terms = nullptr;  // single-query staging (abf_query)
     uint64_t* q_off = nullptr;
+    uint32_t spin_limit = abf::kDefaultSpinLimit;  // polls of every bounded device wait
 };
 
 struct abf_worker {
@@ -333,10 +332,8 @@ void ws_release(abf_workspace* w) {
     dev_free(w->probe_list);
     dev_free(w->n_probe);
     dev_free(w->probe_bm);
-    dev_free(w->counts);
-    dev_free(w->offsets);
     dev_free(w->scan_status);
-    dev_free(w->scan_counter);
+    dev_free(w->ticket);
     dev_free(w->id_off);
     dev_free(w->path_out);
     dev_free(w->auto_paths);
@@ -345,6 +342,8 @@ void ws_release(abf_workspace* w) {
     dev_free(w->q_ndense);
     dev_free(w->q_dmode);
     dev_free(w->err);
+    dev_free(w->tile_list);
+    dev_free(w->n_tile_list);
     dev_free(w->q_terms);
     dev_free(w->q_off);
 }
@@ -363,14 +362,14 @@ abf_status ws_alloc(abf_index* ix, uint32_t max_q, uint64_t max_terms, uint64_t 
         (st = dev_alloc(&w->lcnt, max_q)) != ABF_OK || (st = dev_alloc(&w->lpref_q, uint64_t(max_q) + 1)) != ABF_OK ||
         (st = dev_alloc(&w->probe_list, w->probe_cap)) != ABF_OK || (st = dev_alloc(&w->n_probe, 1)) != ABF_OK ||
         (st = dev_alloc(&w->probe_bm, uint64_t(w->probe_cap) * w->probe_stride)) != ABF_OK ||
-        (st = dev_alloc(&w->counts, chunks)) != ABF_OK || (st = dev_alloc(&w->offsets, chunks + 1)) != ABF_OK ||
-        (st = dev_alloc(&w->scan_status, abf::scan_tiles(chunks))) != ABF_OK ||
-        (st = dev_alloc(&w->scan_counter, 1)) != ABF_OK || (st = dev_alloc(&w->id_off, uint64_t(max_q) + 1)) != ABF_OK ||
+        (st = dev_alloc(&w->scan_status, chunks + 1)) != ABF_OK || (st = dev_alloc(&w->ticket, 1)) != ABF_OK ||
+        (st = dev_alloc(&w->id_off, uint64_t(max_q) + 1)) != ABF_OK ||
         (st = dev_alloc(&w->path_out, max_q)) != ABF_OK || (st = dev_alloc(&w->err, 1)) != ABF_OK ||
         (st = dev_alloc(&w->auto_paths, max_q)) != ABF_OK ||
         (st = dev_alloc(&w->q_dense16, max_terms + 8ull * max_q + 16)) != ABF_OK ||
         (st = dev_alloc(&w->q_dstart, max_q)) != ABF_OK || (st = dev_alloc(&w->q_ndense, max_q)) != ABF_OK ||
-        (st = dev_alloc(&w->q_dmode, max_q)) != ABF_OK ||
+        (st = dev_alloc(&w->q_dmode, max_q)) != ABF_OK || (st = dev_alloc(&w->tile_list, max_q)) != ABF_OK ||
+        (st = dev_alloc(&w->n_tile_list, 1)) != ABF_OK ||
         (st = dev_alloc(&w->q_terms, max_terms)) != ABF_OK || (st = dev_alloc(&w->q_off, 2)) != ABF_OK) {
         ws_release(w);
         return st;
@@ -413,9 +412,7 @@ struct RunOpts {
 };
 
 abf_status run_compact(abf_index* ix, const abf::CompactArgs& ca, cudaStream_t s) {
-    TIMED(K_COUNT, abf::launch_compact_count(ca, ix->sm_count, s));
-    TIMED(K_SCAN, abf::launch_compact_scan(ca, s));
-    TIMED(K_WRITE, abf::launch_compact_write(ca, ix->sm_count, s));
+    TIMED(K_COMPACT, abf::launch_compact(ca, ix->sm_count, s));
     return ABF_OK;
 }
 
@@ -430,6 +427,7 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
     const abf::IndexView v = abf::view_of(ix);
     const abf_tuning& t = ix->tuning;
     CUDA_TRY(cudaMemsetAsync(ws->n_probe, 0, sizeof(uint32_t), s));
+    CUDA_TRY(cudaMemsetAsync(ws->n_tile_list, 0, sizeof(uint32_t), s));
     abf::PlanArgs pa{};
     pa.terms = b->d_terms;
     pa.q_off = b->d_offsets;
@@ -453,6 +451,8 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
     pa.q_dstart = ws->q_dstart;
     pa.q_ndense = ws->q_ndense;
     pa.q_dmode = ws->q_dmode;
+    pa.tile_list = ws->tile_list;
+    pa.n_tile_list = ws->n_tile_list;
     if (!b->d_paths && b->path == ABF_PATH_AUTO && ix->dev.planner) {
         // learned planner: per-query path from the fused feature + MLP kernel
         TIMED(K_PLANNER, abf::launch_planner(v, ix->dev.planner, b->d_terms, b->d_offsets, b->n_queries,
@@ -495,6 +495,8 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
     ta.q_dstart = ws->q_dstart;
     ta.q_ndense = ws->q_ndense;
     ta.q_dmode = ws->q_dmode;
+    ta.tile_list = ws->tile_list;
+    ta.n_tile_list = ws->n_tile_list;
     // dense group kernel: the dense lists of every non-probe query in one pass per
     // tile, when the batch is large enough and the dense bitmaps (plus the
     // zero row) fit three TMA boxes of 256. Tiles of 64 words (two per lane:
@@ -541,6 +543,7 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
         ga.out_stride = b->bitmap_stride_words;
         ga.n_words = n_words;
         ga.err = ws->err;
+        ga.spin_limit = ws->spin_limit;
         TIMED(K_GROUP, abf::launch_dense_group(ix->dense_tmap, gw, ga, ix->sm_count, s));
     }
     TIMED(K_TILE, abf::launch_tile_union(v, ta, tt, ix->sm_count, s));
@@ -567,6 +570,7 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
         pr.out_stride = b->bitmap_stride_words;
         pr.chunk_blocks = t.probe_chunk_blocks;
         pr.err = ws->err;
+        pr.spin_limit = ws->spin_limit;
         TIMED(K_PROBE, abf::launch_probe(v, pr, t, ix->sm_count, s));
     }
     if (b->d_ids || ro.id_counts) {
@@ -576,15 +580,14 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
         ca.n_q = b->n_queries;
         ca.n_bits = ix->n_ads;
         ca.n_chunks = abf::compact_chunks(ix->n_ads);
-        ca.counts = ws->counts;
-        ca.offsets = ws->offsets;
-        ca.scan_status = ws->scan_status;
-        ca.scan_counter = ws->scan_counter;
+        ca.status = ws->scan_status;
+        ca.ticket = ws->ticket;
         ca.ids = b->d_ids;
         ca.capacity = b->d_ids ? b->ids_capacity : 0;
         ca.id_offsets = b->d_id_offsets ? b->d_id_offsets : ws->id_off;
         ca.id_counts = ro.id_counts;
         ca.err = ws->err;
+        ca.spin_limit = ws->spin_limit;
         ABF_TRY(run_compact(ix, ca, s));
     }
     return ABF_OK;
@@ -702,6 +705,7 @@ abf_status run_dense(const abf_worker* w, uint32_t* d_res, uint64_t res_stride_w
     abf_workspace* ws = nullptr;
     ABF_TRY(own_ws(ix, 1, 1, ix->n_ads, &ws));
     pr.err = ws->err;
+    pr.spin_limit = ws->spin_limit;
     TIMED(K_PROBE, abf::launch_probe(abf::view_of(ix), pr, ix->tuning, ix->sm_count, s));
     return ABF_OK;
 }
@@ -1115,15 +1119,14 @@ abf_status abf_collect_ids(abf_index* ix, const uint32_t* d_bitmap, uint64_t n_b
     ca.n_q = 1;
     ca.n_bits = n_bits;
     ca.n_chunks = abf::compact_chunks(n_bits);
-    ca.counts = ws->counts;
-    ca.offsets = ws->offsets;
-    ca.scan_status = ws->scan_status;
-    ca.scan_counter = ws->scan_counter;
+    ca.status = ws->scan_status;
+    ca.ticket = ws->ticket;
     ca.ids = d_ids;
     ca.capacity = ids_capacity;
     ca.id_offsets = ws->id_off;
     ca.id_counts = d_count;
     ca.err = ws->err;
+    ca.spin_limit = ws->spin_limit;
     ABF_TRY(run_compact(ix, ca, static_cast<cudaStream_t>(stream)));
     return ABF_OK;
     API_END
@@ -1183,6 +1186,23 @@ abf_status abf_workspace_check(abf_workspace* w, void* stream) {
     CUDA_TRY(cudaStreamSynchronize(s));
     if (err & abf::kErrTermRange) return fail(ABF_ERR_CAPACITY, "a query's term offsets exceed the workspace's max_terms");
     if (err) return fail(ABF_ERR_TIMEOUT, "a bounded device wait gave up (code " + std::to_string(err) + ")");
+    return ABF_OK;
+    API_END
+}
+
+abf_status abf_workspace_set_wait_limit(abf_workspace* w, uint32_t polls) {
+    if (!w || polls == 0) return fail(ABF_ERR_INVALID, "abf_workspace_set_wait_limit: null workspace or zero polls");
+    w->spin_limit = polls;
+    return ABF_OK;
+}
+
+abf_status abf_workspace_selftest_waits(abf_workspace* w, uint32_t polls, void* stream) {
+    API_BEGIN
+    if (!w || polls == 0) return fail(ABF_ERR_INVALID, "abf_workspace_selftest_waits: null workspace or zero polls");
+    CUDA_TRY(cudaSetDevice(w->ix->device));
+    // the first two look-back words of the compaction scratch (a workspace
+    // has one per chunk of every query, plus one)
+    CUDA_TRY(abf::launch_wait_selftest(w->scan_status, w->err, polls, static_cast<cudaStream_t>(stream)));
     return ABF_OK;
     API_END
 }

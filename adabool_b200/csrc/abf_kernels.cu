@@ -26,10 +26,10 @@ namespace {
 
 constexpr uint32_t kFull = 0xffffffffu;
 constexpr uint32_t kProbeSmemWords = 8192;  // staged term-bitmap words per CTA
-constexpr uint64_t kFlagAgg = 1ull << 62;
-constexpr uint64_t kFlagIncl = 2ull << 62;
+// look-back status word: flag in the top two bits, count below
+constexpr uint64_t kFlagAgg = 1ull << 62;   // the item's own id count is known
+constexpr uint64_t kFlagIncl = 2ull << 62;  // the ids of the item and all before it
 constexpr uint64_t kValMask = (1ull << 62) - 1;
-constexpr uint32_t kSpinLimit = 1u << 22;
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 __device__ __forceinline__ uint32_t warp_id() { return threadIdx.x >> 5; }
@@ -234,6 +234,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
+// Waits for the phase of `bar` with the given parity; false after `limit`
+// polls without it completing.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint32_t limit) {
+    for (uint32_t spins = 0; !mbar_try_wait(bar, parity);)
+        if (++spins > limit) return false;
+    return true;
+}
 
 // ---------------------------------------------------------------------------
 // planning
@@ -339,7 +346,9 @@ __global__ void __launch_bounds__(256) plan_kernel(IndexView ix, PlanArgs a) {
                 a.q_ndense[q] = nd;
                 // 1: every list it merges has a dense bitmap; 2: it also merges
                 // lists without one; 0: probe or empty (no dense merge at all)
-                a.q_dmode[q] = (!probe && qe > qb) ? (any_merge ? 2u : 1u) : 0u;
+                const uint32_t dmode = (!probe && qe > qb) ? (any_merge ? 2u : 1u) : 0u;
+                a.q_dmode[q] = dmode;
+                if (a.tile_list && dmode != 1u) a.tile_list[atomicAdd(a.n_tile_list, 1u)] = q;
             }
         }
         if (tid == 0) {
@@ -489,14 +498,19 @@ __global__ void __launch_bounds__(NW * 32) tile_union_kernel(IndexView ix, TileA
     __shared__ uint32_t s_warp[32];
     __shared__ uint32_t s_ndense;
     const uint32_t tid = threadIdx.x, warp = warp_id();
-    const uint64_t items = uint64_t(a.n_q) * a.n_tiles;
+    // with the dense group kernel writing the dense-only queries, only the
+    // plan kernel's list of the other queries is visited (often none)
+    const bool listed = a.skip_dense_only && a.tile_list;
+    const uint32_t n_q = listed ? *a.n_tile_list : a.n_q;
+    const uint64_t items = uint64_t(n_q) * a.n_tiles;
     uint4* tile4 = reinterpret_cast<uint4*>(tile);
     for (uint64_t item = blockIdx.x; item < items; item += gridDim.x) {
         // tile-major order: the CTAs resident together work on one region of
         // the ad space for many queries, so the blocks and dense slices of
         // lists those queries share are read from L2
-        const uint32_t t = uint32_t(item / a.n_q);
-        const uint32_t q = uint32_t(item - uint64_t(t) * a.n_q);
+        const uint32_t t = uint32_t(item / n_q);
+        const uint32_t qi = uint32_t(item - uint64_t(t) * n_q);
+        const uint32_t q = listed ? a.tile_list[qi] : qi;
         const uint32_t lo_id = t * SPAN;
         const uint32_t hi_id = (uint64_t(lo_id) + SPAN > ix.n_ads) ? ix.n_ads : lo_id + SPAN;
         const uint32_t dj0 = lo_id >> kDirShift;
@@ -720,7 +734,7 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
     extern __shared__ uint8_t g_raw[];
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ uint32_t s_next[2];
-    __shared__ uint32_t s_fail, s_ndq;
+    __shared__ uint32_t s_ndq;
     __shared__ uint32_t s_warp[32];
     uint8_t* base = g_raw + ((1024u - (smem_addr(g_raw) & 1023u)) & 1023u);
     const uint32_t stage_bytes = (a.n_rows * GW * 4u + 1023u) & ~1023u;
@@ -748,7 +762,6 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
         mbar_init(&bar[1], 1);
         fence_mbar_init();
         s_next[0] = s_next[1] = 0;
-        s_fail = 0;
         issue(t, 0);  // the first tile's copy overlaps the list staging below
     }
     // stage those queries' lists (the same for every tile): offsets
@@ -797,24 +810,22 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
     for (uint32_t it = 0; t < a.n_tiles; ++it, t += gridDim.x) {
         const uint32_t st = dbl ? (it & 1u) : 0u;
         const bool more = t + gridDim.x < a.n_tiles;
-        if (tid == 0 && more && dbl) issue(t + gridDim.x, st ^ 1u);
-        uint32_t spins = 0;
-        while (!mbar_try_wait(&bar[st], (phase >> st) & 1u)) {
-            if (++spins > kSpinLimit) {
-                s_fail = 1;
-                break;
-            }
-        }
-        phase ^= 1u << st;
-        if (__syncthreads_or(s_fail)) {
+        const uint32_t par = (phase >> st) & 1u;
+        const bool ok = mbar_wait_bounded(&bar[st], par, a.spin_limit);
+        if (__syncthreads_or(!ok)) {
+            // The copy into this stage is the only one in flight: the next
+            // tile's copy is issued only after a wait succeeds. It gets one
+            // more bounded interval to land before the CTA (and its shared
+            // memory) goes; a copy still pending after that is abandoned
+            // with the error bit set.
             if (tid == 0) atomicOr(a.err, kErrTmaTimeout);
-            if (more && dbl) {  // let the other stage's copy land before the CTA leaves
-                uint32_t sp = 0;
-                while (!mbar_try_wait(&bar[st ^ 1u], (phase >> (st ^ 1u)) & 1u) && ++sp < kSpinLimit) {
-                }
-            }
+            mbar_wait_bounded(&bar[st], par, a.spin_limit);
             return;
         }
+        phase ^= 1u << st;
+        // the other stage was released by the barrier that ended the previous
+        // tile: its refill overlaps this tile's merge
+        if (tid == 0 && more && dbl) issue(t + gridDim.x, st ^ 1u);
         const uint32_t* S = stage0 + st * (stage_bytes / 4u);
         const uint8_t* B = reinterpret_cast<const uint8_t*>(S + lane * kLaneWords);
         const uint64_t w = uint64_t(t) * GW + lane * kLaneWords;
@@ -924,7 +935,6 @@ __global__ void __launch_bounds__(NW * 32) probe_kernel(IndexView ix, ProbeArgs 
     __shared__ __align__(128) uint32_t sbm[kProbeSmemWords];
     __shared__ __align__(16) uint4 stage[NW][32];
     __shared__ __align__(8) uint64_t bar;
-    __shared__ uint32_t s_fail;
     const uint32_t tid = threadIdx.x, lane = lane_id(), warp = warp_id();
     // the device counter also counts queries demoted past the slot capacity
     uint32_t n_probe = a.n_probe_host;
@@ -933,7 +943,6 @@ __global__ void __launch_bounds__(NW * 32) probe_kernel(IndexView ix, ProbeArgs 
     if (tid == 0) {
         mbar_init(&bar, 1);
         fence_mbar_init();
-        s_fail = 0;
     }
     __syncthreads();
     uint32_t phase = 0;
@@ -958,18 +967,16 @@ __global__ void __launch_bounds__(NW * 32) probe_kernel(IndexView ix, ProbeArgs 
                     for (uint32_t g = 0; g < G; ++g)
                         bulk_g2s(sbm + g * span, a.qbm + uint64_t(g0 + g) * a.qbm_stride + w0, span * 4u, &bar);
                 }
-                uint32_t spins = 0;
-                while (!mbar_try_wait(&bar, phase)) {
-                    if (++spins > kSpinLimit) {
-                        s_fail = 1;
-                        break;
-                    }
-                }
-                phase ^= 1u;
-                if (__syncthreads_or(s_fail)) {
+                const bool ok = mbar_wait_bounded(&bar, phase, a.spin_limit);
+                if (__syncthreads_or(!ok)) {
+                    // one more bounded interval for the copies to land before
+                    // the CTA's shared memory is released; copies still
+                    // pending after it are abandoned with the error bit set
                     if (tid == 0) atomicOr(a.err, kErrTmaTimeout);
+                    mbar_wait_bounded(&bar, phase, a.spin_limit);
                     return;
                 }
+                phase ^= 1u;
             }
             for (uint64_t base = c0 + uint64_t(warp) * 128u; base < c1; base += uint64_t(NW) * 128u) {
                 const uint64_t idx = base + lane * 4u;
@@ -1023,7 +1030,7 @@ __global__ void __launch_bounds__(NW * 32) probe_kernel(IndexView ix, ProbeArgs 
 }
 
 // ---------------------------------------------------------------------------
-// compaction: count, decoupled look-back scan, write
+// compaction: one pass (chunk popcount, decoupled look-back, id writes)
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t masked_word(const uint32_t* bm, uint64_t w, uint64_t n_bits) {
     uint32_t v = bm[w];
@@ -1032,113 +1039,68 @@ __device__ __forceinline__ uint32_t masked_word(const uint32_t* bm, uint64_t w, 
     return v;
 }
 
-// Set bits per 2048-word chunk. A full, 16-byte aligned chunk is read with
-// two 16-byte loads per thread; the warps' sums meet in a shared array
-// double-buffered by chunk parity, so a chunk costs one barrier.
-__global__ void __launch_bounds__(256) count_kernel(CompactArgs a) {
-    static_assert(kCompactChunkWords == 256 * 8, "two uint4 per thread");
-    __shared__ uint32_t s_red[2][8];
-    const uint32_t tid = threadIdx.x, lane = lane_id(), warp = warp_id();
-    const uint64_t n_words = (a.n_bits + 31) / 32;
-    const uint64_t items = uint64_t(a.n_q) * a.n_chunks;
-    uint32_t parity = 0;
-    for (uint64_t item = blockIdx.x; item < items; item += gridDim.x, parity ^= 1u) {
-        const uint32_t q = uint32_t(item / a.n_chunks);
-        const uint32_t c = uint32_t(item - uint64_t(q) * a.n_chunks);
-        const uint32_t* bm = a.bm + uint64_t(q) * a.stride;
-        const uint64_t w0 = uint64_t(c) * kCompactChunkWords;
-        uint32_t s = 0;
-        if ((w0 + kCompactChunkWords) * 32u <= a.n_bits && (reinterpret_cast<uintptr_t>(bm + w0) & 15u) == 0) {
-            const uint4* p = reinterpret_cast<const uint4*>(bm + w0);
-            const uint4 x0 = p[tid], x1 = p[tid + 256u];
-            s = __popc(x0.x) + __popc(x0.y) + __popc(x0.z) + __popc(x0.w) + __popc(x1.x) + __popc(x1.y) +
-                __popc(x1.z) + __popc(x1.w);
-        } else {
-            const uint64_t w1 = w0 + kCompactChunkWords < n_words ? w0 + kCompactChunkWords : n_words;
-            for (uint64_t w = w0 + tid; w < w1; w += 256) s += __popc(masked_word(bm, w, a.n_bits));
-        }
-        s = __reduce_add_sync(kFull, s);
-        if (lane == 0) s_red[parity][warp] = s;
-        __syncthreads();
-        if (warp == 0) {
-            uint32_t t = lane < 8u ? s_red[parity][lane] : 0u;
-            t = __reduce_add_sync(kFull, t);
-            if (lane == 0) a.counts[item] = t;
-        }
-    }
+__device__ __forceinline__ uint64_t ld_status(const uint64_t* p) {
+    return *reinterpret_cast<const volatile unsigned long long*>(p);
+}
+__device__ __forceinline__ void st_status(uint64_t* p, uint64_t v) {
+    __threadfence();
+    atomicExch(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(v));
 }
 
-constexpr int kScanNT = 256;
-constexpr int kScanIPT = int(kScanTile) / kScanNT;
-
-__global__ void __launch_bounds__(kScanNT) scan_kernel(const uint32_t* in, uint64_t n, uint64_t* out, uint64_t* status,
-                                                      uint32_t* counter, uint32_t* err) {
-    __shared__ uint32_t s_tile;
-    __shared__ unsigned long long s_prefix;
-    __shared__ uint32_t s_warp[32];
-    const uint32_t tid = threadIdx.x;
-    if (tid == 0) s_tile = atomicAdd(counter, 1u);
-    __syncthreads();
-    const uint64_t tile = s_tile;
-    const uint64_t base = tile * kScanTile + uint64_t(tid) * kScanIPT;
-    uint32_t v[kScanIPT];
-    uint32_t sum = 0;
-#pragma unroll
-    for (int k = 0; k < kScanIPT; ++k) {
-        v[k] = base + k < n ? in[base + k] : 0u;
-        sum += v[k];
+// Decoupled look-back, run by one whole warp for work item `item` whose own
+// id count is `agg`: publishes the count, then reads the status words of the
+// earlier items 32 at a time (lane k reads item - 1 - k of the window),
+// waits until none of them is empty, and adds up the counts back to the
+// nearest item that has published its inclusive prefix; publishes its own
+// inclusive prefix and returns the exclusive one in *excl. Items are claimed
+// in ascending order by running CTAs, each of which publishes its count
+// before it looks back, so every wait ends; a wait that still sees an empty
+// word after `limit` polls gives up and returns false.
+__device__ bool lookback_prefix(uint64_t* status, uint64_t item, uint32_t agg, uint32_t limit, uint64_t* excl) {
+    const uint32_t lane = lane_id();
+    if (item == 0) {
+        if (lane == 0) st_status(status, kFlagIncl | agg);
+        *excl = 0;
+        return true;
     }
-    uint32_t agg;
-    const uint32_t ex = block_excl_scan<kScanNT>(sum, s_warp, &agg);
-    if (tid == 0) {
-        uint64_t prefix = 0;
-        if (tile == 0) {
-            __threadfence();
-            atomicExch(reinterpret_cast<unsigned long long*>(status), (unsigned long long)(kFlagIncl | agg));
-        } else {
-            __threadfence();
-            atomicExch(reinterpret_cast<unsigned long long*>(status + tile), (unsigned long long)(kFlagAgg | agg));
-            uint64_t k = tile - 1;
-            uint32_t spins = 0;
-            for (;;) {
-                const uint64_t s = *reinterpret_cast<volatile unsigned long long*>(status + k);
-                const uint64_t f = s & ~kValMask;
-                if (f == 0) {
-                    if (++spins > kSpinLimit) {
-                        atomicOr(err, kErrScanTimeout);
-                        break;
-                    }
-                    __nanosleep(32);
-                    continue;
-                }
-                prefix += s & kValMask;
-                if (f == kFlagIncl || k == 0) break;
-                --k;
+    if (lane == 0) st_status(status + item, kFlagAgg | agg);
+    uint64_t prefix = 0;
+    uint64_t end = item;  // the window is items [end - 32, end)
+    uint32_t spins = 0;
+    for (;;) {
+        const bool in_range = end > uint64_t(lane);
+        const uint64_t sw = in_range ? ld_status(status + (end - 1u - lane)) : kFlagIncl;  // before item 0: 0
+        if (__any_sync(kFull, (sw >> 62) == 0u)) {
+            if (++spins > limit) {
+                *excl = prefix;
+                return false;
             }
-            __threadfence();
-            atomicExch(reinterpret_cast<unsigned long long*>(status + tile),
-                       (unsigned long long)(kFlagIncl | (prefix + agg)));
+            __nanosleep(64);
+            continue;
         }
-        s_prefix = prefix;
-    }
-    __syncthreads();
-    uint64_t run = s_prefix + ex;
+        const uint32_t incl = __ballot_sync(kFull, (sw >> 62) == 2u);
+        const uint32_t upto = incl ? uint32_t(__ffs(incl)) - 1u : 31u;  // nearest inclusive word in the window
+        uint64_t v = lane <= upto ? (sw & kValMask) : 0ull;
 #pragma unroll
-    for (int k = 0; k < kScanIPT; ++k) {
-        if (base + k < n) out[base + k] = run;
-        run += v[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+        prefix += v;
+        if (incl) break;
+        end -= 32u;
     }
-    const uint64_t last_tile = (n - 1) / kScanTile;
-    if (tile == last_tile && tid == 0) out[n] = s_prefix + agg;
+    if (lane == 0) st_status(status + item, kFlagIncl | (prefix + agg));
+    *excl = prefix;
+    return true;
 }
 
-// One CTA per (bitmap, 2048-word chunk) at a time; each of its 8 warps owns
-// 8 consecutive units of 32 words, held in registers (lane l: word l of
-// each unit). One barrier per chunk exchanges the warps' id totals; then
-// every warp expands its units on its own, one word at a time with one lane
-// per bit: the lanes holding set bits store their ids to consecutive output
-// addresses (rank = popcount of the lower bits), so each store instruction
-// writes one contiguous run and no lane loops over bits.
+// One CTA per (bitmap, 2048-word chunk) at a time, items taken in ascending
+// order from a ticket counter. Each of the 8 warps owns 8 consecutive units
+// of 32 words, held in registers (lane l: word l of each unit); their
+// popcounts give the chunk's id count, warp 0 looks back for the chunk's
+// output offset, and then every warp expands its units on its own, one word
+// at a time with one lane per bit: the lanes holding set bits store their
+// ids to consecutive output addresses (rank = popcount of the lower bits), so
+// each store instruction writes one contiguous run and no lane loops over
+// bits. The bitmap is read once: there is no separate counting pass.
 constexpr uint32_t kUnits = kCompactChunkWords / 32;
 constexpr uint32_t kWarpUnits = kUnits / 8;
 static_assert(kUnits == 64, "8 warps x 8 units cover one chunk");
@@ -1187,26 +1149,24 @@ __device__ __forceinline__ void expand_unit(uint32_t v, uint32_t ex, uint32_t id
     }
 }
 
-__global__ void __launch_bounds__(256) write_ids_kernel(CompactArgs a) {
+__global__ void __launch_bounds__(256) compact_kernel(CompactArgs a) {
     __shared__ __align__(16) uint32_t s_buf[8][kIdBuf];
-    __shared__ uint32_t s_wtot[2][8];  // per-warp id totals, double-buffered by chunk parity
+    __shared__ uint32_t s_wtot[8];
+    __shared__ unsigned long long s_item, s_prefix;
     const uint32_t lane = lane_id(), warp = warp_id();
     const uint32_t lt = lanemask_lt(), mybit = 1u << lane;
     const bool ids16 = (reinterpret_cast<uintptr_t>(a.ids) & 15u) == 0;
     uint32_t* buf = s_buf[warp];
     const uint64_t n_words = (a.n_bits + 31) / 32;
     const uint64_t items = uint64_t(a.n_q) * a.n_chunks;
-    uint32_t parity = 0;
-    for (uint64_t item = blockIdx.x; item < items; item += gridDim.x, parity ^= 1u) {
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(a.ticket, 1ull);
+        __syncthreads();
+        const uint64_t item = s_item;
+        if (item >= items) break;
         const uint32_t q = uint32_t(item / a.n_chunks);
         const uint32_t c = uint32_t(item - uint64_t(q) * a.n_chunks);
         const uint32_t* bm = a.bm + uint64_t(q) * a.stride;
-        const uint64_t out = a.offsets[item];
-        if (c == 0 && threadIdx.x == 0) {
-            if (a.id_offsets) a.id_offsets[q] = out;
-            if (a.id_counts) a.id_counts[q] = a.offsets[item + a.n_chunks] - out;
-            if (a.id_offsets && q == a.n_q - 1) a.id_offsets[a.n_q] = a.offsets[items];
-        }
         const uint64_t wbase = uint64_t(c) * kCompactChunkWords + uint64_t(warp) * (kWarpUnits * 32u);
         uint32_t v[kWarpUnits], tot[kWarpUnits];
 #pragma unroll
@@ -1220,9 +1180,24 @@ __global__ void __launch_bounds__(256) write_ids_kernel(CompactArgs a) {
             tot[k] = __reduce_add_sync(kFull, uint32_t(__popc(v[k])));
             wsum += tot[k];
         }
-        if (lane == 0) s_wtot[parity][warp] = wsum;
+        if (lane == 0) s_wtot[warp] = wsum;
         __syncthreads();
-        uint64_t o0 = out + __reduce_add_sync(kFull, lane < warp ? s_wtot[parity][lane] : 0u);
+        if (warp == 0) {
+            const uint32_t t = __reduce_add_sync(kFull, lane < 8u ? s_wtot[lane] : 0u);
+            uint64_t excl = 0;
+            const bool ok = lookback_prefix(a.status, item, t, a.spin_limit, &excl);
+            if (lane == 0) {
+                if (!ok) atomicOr(a.err, kErrScanTimeout);
+                s_prefix = excl;
+                if (a.id_offsets) {
+                    if (c == 0) a.id_offsets[q] = excl;
+                    if (item + 1 == items) a.id_offsets[a.n_q] = excl + t;
+                }
+                if (a.id_counts && t) atomicAdd(reinterpret_cast<unsigned long long*>(a.id_counts + q), t);
+            }
+        }
+        __syncthreads();
+        uint64_t o0 = s_prefix + __reduce_add_sync(kFull, lane < warp ? s_wtot[lane] : 0u);
 #pragma unroll
         for (uint32_t k = 0; k < kWarpUnits; ++k) {
             const uint32_t t = tot[k];
@@ -1275,6 +1250,31 @@ __global__ void __launch_bounds__(256) write_ids_kernel(CompactArgs a) {
     if (lane == 0) bulk_wait_all();
 }
 
+// ---------------------------------------------------------------------------
+// self-test of the bounded waits
+// ---------------------------------------------------------------------------
+// CTA 0 arms an mbarrier for 16 bytes that no copy delivers and waits on it
+// with mbar_wait_bounded; CTA 1 looks back from item 1 at status[0], which
+// nothing publishes, with lookback_prefix. No asynchronous copy is ever
+// issued, so nothing is in flight when the CTAs leave.
+__global__ void __launch_bounds__(32) wait_selftest_kernel(uint64_t* status2, uint32_t* err, uint32_t limit) {
+    __shared__ __align__(8) uint64_t bar;
+    if (blockIdx.x == 0) {
+        if (threadIdx.x == 0) {
+            mbar_init(&bar, 1);
+            fence_mbar_init();
+            mbar_expect_tx(&bar, 16u);
+        }
+        __syncwarp();
+        const bool ok = mbar_wait_bounded(&bar, 0u, limit);
+        if (__any_sync(kFull, !ok) && threadIdx.x == 0) atomicOr(err, kErrTmaTimeout);
+    } else {
+        uint64_t excl = 0;
+        const bool ok = lookback_prefix(status2, 1u, 7u, limit, &excl);
+        if (!ok && threadIdx.x == 0) atomicOr(err, kErrScanTimeout);
+    }
+}
+
 inline int grid_for(uint64_t items, int sm_count, uint32_t per_sm) {
     uint64_t g = uint64_t(sm_count) * (per_sm ? per_sm : 1u);
     if (items < g) g = items;
@@ -1310,7 +1310,6 @@ uint32_t compact_chunks(uint64_t n_bits) {
     const uint64_t n_words = (n_bits + 31) / 32;
     return uint32_t((n_words + kCompactChunkWords - 1) / kCompactChunkWords);
 }
-uint64_t scan_tiles(uint64_t n) { return (n + kScanTile - 1) / kScanTile; }
 
 cudaError_t launch_plan(const IndexView& v, const PlanArgs& a, cudaStream_t s) {
     if (a.n_q == 0) return cudaSuccess;
@@ -1489,32 +1488,22 @@ cudaError_t launch_probe(const IndexView& v, const ProbeArgs& a, const abf_tunin
     return cudaGetLastError();
 }
 
-cudaError_t launch_compact_count(const CompactArgs& a, int sm_count, cudaStream_t s) {
+cudaError_t launch_compact(const CompactArgs& a, int sm_count, cudaStream_t s) {
     const uint64_t items = uint64_t(a.n_q) * a.n_chunks;
     if (items == 0) return cudaSuccess;
-    count_kernel<<<grid_for(items, sm_count, 8), 256, 0, s>>>(a);
+    cudaError_t e = cudaMemsetAsync(a.status, 0, items * sizeof(uint64_t), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(a.ticket, 0, sizeof(unsigned long long), s);
+    if (e == cudaSuccess && a.id_counts) e = cudaMemsetAsync(a.id_counts, 0, uint64_t(a.n_q) * sizeof(uint64_t), s);
+    if (e != cudaSuccess) return e;
+    compact_kernel<<<grid_for(items, sm_count, 6), 256, 0, s>>>(a);
     count_launch();
     return cudaGetLastError();
 }
 
-cudaError_t launch_compact_scan(const CompactArgs& a, cudaStream_t s) {
-    const uint64_t items = uint64_t(a.n_q) * a.n_chunks;
-    if (items == 0) return cudaSuccess;
-    const uint64_t tiles = scan_tiles(items);
-    cudaError_t e = cudaMemsetAsync(a.scan_status, 0, tiles * sizeof(uint64_t), s);
+cudaError_t launch_wait_selftest(uint64_t* status2, uint32_t* err, uint32_t spin_limit, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(status2, 0, 2 * sizeof(uint64_t), s);
     if (e != cudaSuccess) return e;
-    e = cudaMemsetAsync(a.scan_counter, 0, sizeof(uint32_t), s);
-    if (e != cudaSuccess) return e;
-    scan_kernel<<<unsigned(tiles), kScanNT, 0, s>>>(a.counts, items, a.offsets, a.scan_status, a.scan_counter,
-                                                    a.err);
-    count_launch();
-    return cudaGetLastError();
-}
-
-cudaError_t launch_compact_write(const CompactArgs& a, int sm_count, cudaStream_t s) {
-    const uint64_t items = uint64_t(a.n_q) * a.n_chunks;
-    if (items == 0) return cudaSuccess;
-    write_ids_kernel<<<grid_for(items, sm_count, 6), 256, 0, s>>>(a);
+    wait_selftest_kernel<<<2, 32, 0, s>>>(status2, err, spin_limit);
     count_launch();
     return cudaGetLastError();
 }

@@ -17,7 +17,9 @@
 //                      the probe queries' term-bitmap slices in shared memory
 //                      with bulk async copies (TMA engine), tests each block's
 //                      term and scatters hit blocks into their queries
-//   count/scan/write   compaction: bitmap -> ascending uint32 ids
+//   compact_kernel     compaction: bitmap -> ascending uint32 ids in one pass
+//                      (chunk popcounts, decoupled look-back prefix, id
+//                      writes)
 #pragma once
 
 #include <cstdint>
@@ -30,12 +32,17 @@ constexpr uint32_t kNoHeavy = 0xffffffffu;   // heavy_min meaning "merge no list
 constexpr uint32_t kDenseOnly = 0xfffffffeu; // heavy_min meaning "merge only the dense-bitmap lists"
 constexpr uint32_t kCompactChunkWords = 2048; // bitmap words per compaction work item
 constexpr uint32_t kProbeGroup = 32;          // probe queries tested per pass
-constexpr uint32_t kScanTile = 2048;          // elements per decoupled look-back tile
 
 // device error codes (workspace flag)
 constexpr uint32_t kErrScanTimeout = 1u;
 constexpr uint32_t kErrTmaTimeout = 2u;
 constexpr uint32_t kErrTermRange = 4u;
+
+// Polls of a bounded device wait (look-back status word, mbarrier) before it
+// gives up, sets its error bit and returns. A look-back poll sleeps ~64 ns,
+// an mbarrier poll is one try_wait (which itself suspends for a
+// hardware-defined interval), so the default allows well over a second.
+constexpr uint32_t kDefaultSpinLimit = 1u << 22;
 
 struct PlanArgs {
     const uint32_t* terms;
@@ -54,6 +61,11 @@ struct PlanArgs {
     uint8_t* path_out;        // out (optional): resolved path per query
     uint64_t max_terms;       // term slots of the scratch arrays; queries past it get no work
     uint32_t* err;            // device error flag (optional)
+    // optional: queries the merge kernel still has to visit when the dense
+    // group kernel writes the dense-only ones (q_dmode != 1), compacted in
+    // any order; n_tile_list is zeroed before launch
+    uint32_t* tile_list;
+    uint32_t* n_tile_list;
     int dense_in_tile;        // 1: dense-bitmap lists go to the merge kernel, 0: scattered too
     uint32_t* tile_cls;       // out: per term slot, what the merge kernel does with it
                               // (kNone: nothing, kDenseFlag | d: dense bitmap d, else the term)
@@ -109,6 +121,10 @@ struct TileArgs {
     const uint32_t* q_ndense;
     const uint32_t* q_dmode;
     int skip_dense_only;
+    // with skip_dense_only: the plan kernel's list of the queries that are
+    // not dense-only (the only ones this kernel visits) and its length
+    const uint32_t* tile_list;
+    const uint32_t* n_tile_list;
 };
 
 // dense group kernel: one pass per 32- or 64-word tile over all dense-only queries
@@ -131,6 +147,7 @@ struct DenseGroupArgs {
     uint64_t out_stride;
     uint64_t n_words;
     uint32_t* err;
+    uint32_t spin_limit;       // polls of an mbarrier wait before it gives up
 };
 
 struct ScatterArgs {
@@ -157,28 +174,31 @@ struct ProbeArgs {
     uint64_t out_stride;
     uint32_t chunk_blocks;     // multiple of 128
     uint32_t* err;
+    uint32_t spin_limit;       // polls of an mbarrier wait before it gives up
 };
 
+// Compaction of n_q bitmaps into one packed id array. Work item i is chunk
+// i % n_chunks of bitmap i / n_chunks; items are claimed in ascending order
+// from a ticket counter, and each publishes its id count in status[i] so
+// that later items find their output offset by looking back.
 struct CompactArgs {
     const uint32_t* bm;
     uint64_t stride;           // words between bitmaps
     uint32_t n_q;
     uint64_t n_bits;           // ids >= n_bits are dropped
     uint32_t n_chunks;         // per bitmap
-    uint32_t* counts;          // n_q * n_chunks
-    uint64_t* offsets;         // n_q * n_chunks + 1
-    uint64_t* scan_status;     // per scan tile
-    uint32_t* scan_counter;
+    uint64_t* status;          // n_q * n_chunks look-back words, zeroed before launch
+    unsigned long long* ticket;  // item counter, zeroed before launch
     uint32_t* ids;
     uint64_t capacity;
     uint64_t* id_offsets;      // optional n_q + 1
-    uint64_t* id_counts;       // optional n_q
+    uint64_t* id_counts;       // optional n_q, accumulated (zeroed before launch)
     uint32_t* err;
+    uint32_t spin_limit;       // polls of a look-back wait before it gives up
 };
 
 IndexView view_of(const abf_index* ix);
 uint32_t compact_chunks(uint64_t n_bits);
-uint64_t scan_tiles(uint64_t n);
 
 cudaError_t launch_plan(const IndexView& v, const PlanArgs& a, cudaStream_t s);
 // two 2-D TMA descriptors (2 x 128 bytes into out) of the dense bitmaps:
@@ -209,8 +229,14 @@ cudaError_t launch_mlp_grad(const float* p, const float* x, const float* t, cons
 cudaError_t launch_adam(float* p, const float* g, float* m, float* v, uint32_t step, float lr, float b1, float b2,
                         float eps, cudaStream_t s);
 
-cudaError_t launch_compact_count(const CompactArgs& a, int sm_count, cudaStream_t s);
-cudaError_t launch_compact_scan(const CompactArgs& a, cudaStream_t s);
-cudaError_t launch_compact_write(const CompactArgs& a, int sm_count, cudaStream_t s);
+// clears status / ticket / id_counts on the stream, then one compaction launch
+cudaError_t launch_compact(const CompactArgs& a, int sm_count, cudaStream_t s);
+
+// Self-test of the bounded waits: one CTA arms an mbarrier for 16 bytes that
+// no copy delivers, another looks back at a status word that no item
+// publishes (status2[0], zeroed here); both run the same wait code as the
+// path kernels with the given poll limit, give up, set kErrTmaTimeout /
+// kErrScanTimeout in *err and return.
+cudaError_t launch_wait_selftest(uint64_t* status2, uint32_t* err, uint32_t spin_limit, cudaStream_t s);
 
 }  // namespace abf

@@ -6,18 +6,21 @@
 // synchronisation would stall the other streams, or code that must not run
 // into out-of-memory in the middle of a request. This entry point uses no
 // cudaMalloc/cudaFree (and no allocating library call): the compaction's
-// scratch -- per-chunk counts, chunk offsets, the look-back status words --
-// lives in one file-scope device array, sized for bitmaps of at most
-// ABF_NOALLOC_MAX_BITS bits (about 200 KB, held on every device that loads
-// the library until the process exits).
+// scratch -- one look-back status word per 2048-word chunk, the item ticket
+// and an error word -- lives in one file-scope device array, sized for
+// bitmaps of at most ABF_NOALLOC_MAX_BITS bits (about 128 KB, held on every
+// device that loads the library until the process exits).
 //
 // Host code may not pass the array's name to a kernel (on the host it is
 // only a stand-in symbol): the first call on each device looks up its device
 // address with cudaGetSymbolAddress while that device is current and keeps
 // it. That first call should come before any stream capture. All calls on a
 // device share the array and it keeps the last call's contents; the parts
-// that must start at zero are cleared on the stream by every call, and calls
-// whose work overlaps on the GPU (other streams, no ordering) race on it.
+// that must start at zero (status words, ticket, error word) are cleared on
+// the stream by every call, and calls whose work overlaps on the GPU (other
+// streams, no ordering) race on it. abf_collect_ids_noalloc_check reads the
+// error word that the last call on the device left (a look-back wait that
+// gave up).
 #include "abf_kernels.cuh"
 
 #include <mutex>
@@ -27,14 +30,11 @@ namespace {
 
 constexpr uint64_t kMaxBits = ABF_NOALLOC_MAX_BITS;
 constexpr uint64_t kMaxChunks = (kMaxBits / 32 + abf::kCompactChunkWords - 1) / abf::kCompactChunkWords;
-constexpr uint64_t kMaxScanTiles = (kMaxChunks + abf::kScanTile - 1) / abf::kScanTile;
-// layout in 8-byte words: offsets[kMaxChunks + 1], status[kMaxScanTiles],
-// then counts[kMaxChunks] and the scan counter as 4-byte values
-constexpr uint64_t kOffsetsAt = 0;
-constexpr uint64_t kStatusAt = kOffsetsAt + kMaxChunks + 1;
-constexpr uint64_t kCountsAt = kStatusAt + kMaxScanTiles;
-constexpr uint64_t kCounterAt = kCountsAt + (kMaxChunks + 1) / 2;
-constexpr uint64_t kErrAt = kCounterAt + 1;
+// layout in 8-byte words: status[kMaxChunks] (one look-back word per chunk),
+// the item ticket, the error word (low 4 bytes)
+constexpr uint64_t kStatusAt = 0;
+constexpr uint64_t kTicketAt = kStatusAt + kMaxChunks;
+constexpr uint64_t kErrAt = kTicketAt + 1;
 constexpr uint64_t kScratchWords = kErrAt + 1;
 
 static __device__ __align__(256) unsigned long long g_noalloc_scratch[kScratchWords];
@@ -94,23 +94,43 @@ extern "C" abf_status abf_collect_ids_noalloc(const uint32_t* d_bitmap, uint64_t
         ca.n_q = 1;
         ca.n_bits = n_bits;
         ca.n_chunks = abf::compact_chunks(n_bits);
-        ca.offsets = reinterpret_cast<uint64_t*>(b + kOffsetsAt);
-        ca.scan_status = reinterpret_cast<uint64_t*>(b + kStatusAt);
-        ca.counts = reinterpret_cast<uint32_t*>(b + kCountsAt);
-        ca.scan_counter = reinterpret_cast<uint32_t*>(b + kCounterAt);
+        ca.status = reinterpret_cast<uint64_t*>(b + kStatusAt);
+        ca.ticket = b + kTicketAt;
         ca.err = reinterpret_cast<uint32_t*>(b + kErrAt);
         ca.ids = d_ids;
         ca.capacity = ids_capacity;
         ca.id_offsets = nullptr;
         ca.id_counts = d_count;
+        ca.spin_limit = abf::kDefaultSpinLimit;
         cudaStream_t s = static_cast<cudaStream_t>(stream);
-        // the scan clears its status words and tile counter on the stream
-        if ((e = abf::launch_compact_count(ca, slot.sm_count, s)) != cudaSuccess ||
-            (e = abf::launch_compact_scan(ca, s)) != cudaSuccess ||
-            (e = abf::launch_compact_write(ca, slot.sm_count, s)) != cudaSuccess)
+        // the error word starts clear for every call; launch_compact clears
+        // the status words, the ticket and *d_count on the stream
+        if ((e = cudaMemsetAsync(ca.err, 0, sizeof(uint32_t), s)) != cudaSuccess ||
+            (e = abf::launch_compact(ca, slot.sm_count, s)) != cudaSuccess)
             return abf::fail(ABF_ERR_CUDA, std::string("abf_collect_ids_noalloc launch: ") + cudaGetErrorString(e));
         return ABF_OK;
     } catch (...) {
         return abf::fail(ABF_ERR_INTERNAL, "abf_collect_ids_noalloc: unexpected exception");
+    }
+}
+
+extern "C" abf_status abf_collect_ids_noalloc_check(void* stream) {
+    try {
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return abf::fail(ABF_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+        DeviceSlot slot;
+        abf_status st = slot_for(dev, &slot);
+        if (st != ABF_OK) return st;
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        uint32_t err = 0;
+        if ((e = cudaMemcpyAsync(&err, slot.base + kErrAt, sizeof(err), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(s)) != cudaSuccess)
+            return abf::fail(ABF_ERR_CUDA, std::string("abf_collect_ids_noalloc_check: ") + cudaGetErrorString(e));
+        if (err) return abf::fail(ABF_ERR_TIMEOUT, "abf_collect_ids_noalloc: a look-back wait gave up (code " +
+                                                       std::to_string(err) + "); its ids are not valid");
+        return ABF_OK;
+    } catch (...) {
+        return abf::fail(ABF_ERR_INTERNAL, "abf_collect_ids_noalloc_check: unexpected exception");
     }
 }

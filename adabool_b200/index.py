@@ -76,6 +76,15 @@ class Workspace:
     def check(self, stream=None):
         check(lib().abf_workspace_check(self._h, stream_ptr(stream)))
 
+    def set_wait_limit(self, polls: int):
+        """Polls of every bounded device wait of this workspace's kernels."""
+        check(lib().abf_workspace_set_wait_limit(self._h, int(polls)))
+
+    def selftest_waits(self, polls: int, stream=None):
+        """Makes one mbarrier wait and one look-back wait run out (see
+        abf_workspace_selftest_waits); check() then raises ABF_ERR_TIMEOUT."""
+        check(lib().abf_workspace_selftest_waits(self._h, int(polls), stream_ptr(stream)))
+
     def free(self):
         if self._h:
             lib().abf_workspace_free(self._h)

@@ -239,16 +239,24 @@ abf_status abf_collect_ids(abf_index* index, const uint32_t* d_bitmap, uint64_t 
  * to allocate, a serving thread that cannot afford cudaMalloc's possible
  * device-wide synchronisation, code that must not hit out-of-memory in
  * the middle of a request. Needs no index and calls no cudaMalloc/cudaFree:
- * its scratch is one static device array (about 200 KB per device, kept
- * until the process exits) sized for at most ABF_NOALLOC_MAX_BITS bits;
- * larger bitmaps are refused with ABF_ERR_CAPACITY. The first call on a
- * device looks up that array's device address (cudaGetSymbolAddress) and
- * should come before any stream capture. Every call on a device shares the
- * array: calls whose work can overlap on the GPU race and must be ordered
- * by the caller (one stream, or events). Results equal abf_collect_ids. */
+ * its scratch is one static device array (about 128 KB per device, kept
+ * until the process exits) sized for at most ABF_NOALLOC_MAX_BITS bits.
+ * Larger bitmaps are refused with ABF_ERR_CAPACITY -- where abf_collect_ids
+ * refuses only bitmaps above 2^32 bits, with ABF_ERR_RANGE. The first call
+ * on a device looks up that array's device address (cudaGetSymbolAddress)
+ * and should come before any stream capture. Every call on a device shares
+ * the array: calls whose work can overlap on the GPU race and must be
+ * ordered by the caller (one stream, or events). Ids and count equal
+ * abf_collect_ids's. A device-side wait that gave up is reported by
+ * abf_collect_ids_noalloc_check, not by this call's return value. */
 #define ABF_NOALLOC_MAX_BITS (1ull << 30)
 abf_status abf_collect_ids_noalloc(const uint32_t* d_bitmap, uint64_t n_bits, uint32_t* d_ids,
                                    uint64_t ids_capacity, uint64_t* d_count, void* stream);
+/* Synchronises `stream` and reports the error word that the last
+ * abf_collect_ids_noalloc call on the current device left: ABF_ERR_TIMEOUT
+ * if its look-back wait gave up (its ids are then not valid), else ABF_OK.
+ * Each abf_collect_ids_noalloc call clears the word first. */
+abf_status abf_collect_ids_noalloc_check(void* stream);
 
 /* ------------------------------------------------------------------ */
 /* Native batched API (no reference counterpart beyond the batch paths) */
@@ -260,8 +268,28 @@ abf_status abf_collect_ids_noalloc(const uint32_t* d_bitmap, uint64_t n_bits, ui
 abf_status abf_workspace_create(abf_index* index, uint32_t max_queries, uint64_t max_terms,
                                 abf_workspace** out);
 abf_status abf_workspace_free(abf_workspace* ws);
-/* Reads and clears the device error flag (synchronises the stream). */
+/* Reads and clears the device error flag (synchronises the stream):
+ * ABF_ERR_TIMEOUT when a bounded device wait gave up, ABF_ERR_CAPACITY when a
+ * query's term offsets exceeded the workspace. */
 abf_status abf_workspace_check(abf_workspace* ws, void* stream);
+
+/* Bounded device waits. The kernels launched with this workspace poll a
+ * compaction look-back word or an mbarrier at most `polls` times (default
+ * 2^22, well over a second) before they give up, set the workspace's error
+ * flag (abf_workspace_check then returns ABF_ERR_TIMEOUT) and return; no
+ * kernel traps or spins without end. The reference has no device waits (its
+ * kernels are launched back to back, test/adsfilter_q_all.cu:26-105). */
+abf_status abf_workspace_set_wait_limit(abf_workspace* ws, uint32_t polls);
+
+/* Diagnostic of those waits: launches, on `stream`, one CTA that arms an
+ * mbarrier for a copy that is never issued and one that looks back at a
+ * compaction status word that nothing publishes; both wait with the same
+ * device code as the path kernels for at most `polls` polls, give up, set
+ * their bits in the workspace's error flag and return. A following
+ * abf_workspace_check returns ABF_ERR_TIMEOUT, and the context stays usable.
+ * Uses the workspace's compaction scratch: not concurrently with a batch on
+ * the same workspace. No reference counterpart. */
+abf_status abf_workspace_selftest_waits(abf_workspace* ws, uint32_t polls, void* stream);
 
 typedef struct abf_batch {
     const uint32_t* d_terms;     /* flat query terms (device) */
