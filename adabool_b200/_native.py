@@ -151,6 +151,10 @@ PROTOTYPES = {
     "abf_workspace_selftest_waits": [vp, C.c_uint32, vp],
     "abf_batch_run": [vp, vp, C.POINTER(Batch), vp],
     "abf_query": [vp, u32p, C.c_uint32, C.c_int, vp, vp, C.c_uint64, vp, vp],
+    "abf_batch_graph_create": [vp, vp, C.POINTER(Batch), vp, C.POINTER(vp)],
+    "abf_batch_graph_replay": [vp, vp],
+    "abf_batch_graph_kernels": [vp, u32p],
+    "abf_batch_graph_destroy": [vp],
     "abf_planner_features": [vp, vp, vp, C.c_uint32, vp, vp],
     "abf_planner_set": [vp, vp],
     "abf_planner_predict": [vp, vp, vp, C.c_uint32, vp, vp, vp],

@@ -1217,6 +1217,104 @@ abf_status abf_batch_run(abf_index* ix, abf_workspace* ws, const abf_batch* b, v
     API_END
 }
 
+}  // extern "C"
+
+struct abf_batch_graph {
+    abf_index* ix = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint32_t n_kernel_nodes = 0;
+};
+
+extern "C" {
+
+abf_status abf_batch_graph_create(abf_index* ix, abf_workspace* ws, const abf_batch* b, void* stream,
+                                  abf_batch_graph** out) {
+    API_BEGIN
+    ABF_TRY(need_device(ix));
+    if (!ws || !b || !out || ws->ix != ix) return fail(ABF_ERR_INVALID, "abf_batch_graph_create: bad arguments");
+    if (!stream) return fail(ABF_ERR_INVALID, "abf_batch_graph_create: capture needs a created stream, not the default one");
+    if (b->n_queries == 0) return fail(ABF_ERR_INVALID, "abf_batch_graph_create: empty batch");
+    if (!b->d_terms || !b->d_offsets || !b->d_bitmaps) return fail(ABF_ERR_INVALID, "abf_batch_graph_create: null device array");
+    *out = nullptr;
+    CUDA_TRY(cudaSetDevice(ix->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // one direct run first: it makes every host-side setting the batch needs
+    // (kernel attributes, the dense bitmaps' tensor maps), so that the
+    // captured run issues only stream work; no event records in the graph
+    const bool prof = ix->prof_on;
+    ix->prof_on = false;
+    abf_status st = run_batch(ix, ws, b, RunOpts{}, s);
+    if (st != ABF_OK) {
+        ix->prof_on = prof;
+        return st;
+    }
+    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        ix->prof_on = prof;
+        return fail(ABF_ERR_CUDA, std::string("cudaStreamBeginCapture: ") + cudaGetErrorString(e));
+    }
+    st = run_batch(ix, ws, b, RunOpts{}, s);
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(s, &graph);  // always ends the capture, also after a failed run
+    ix->prof_on = prof;
+    if (st != ABF_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return st;
+    }
+    if (e != cudaSuccess) return fail(ABF_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return fail(ABF_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    }
+    auto* g = new abf_batch_graph();
+    g->ix = ix;
+    g->graph = graph;
+    g->exec = exec;
+    size_t n_nodes = 0;
+    if (cudaGraphGetNodes(graph, nullptr, &n_nodes) == cudaSuccess && n_nodes) {
+        std::vector<cudaGraphNode_t> nodes(n_nodes);
+        if (cudaGraphGetNodes(graph, nodes.data(), &n_nodes) == cudaSuccess)
+            for (size_t i = 0; i < n_nodes; ++i) {
+                cudaGraphNodeType ty;
+                if (cudaGraphNodeGetType(nodes[i], &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel)
+                    ++g->n_kernel_nodes;
+            }
+    }
+    *out = g;
+    return ABF_OK;
+    API_END
+}
+
+abf_status abf_batch_graph_replay(abf_batch_graph* g, void* stream) {
+    API_BEGIN
+    if (!g) return fail(ABF_ERR_INVALID, "null graph");
+    CUDA_TRY(cudaSetDevice(g->ix->device));
+    CUDA_TRY(cudaGraphLaunch(g->exec, static_cast<cudaStream_t>(stream)));
+    abf::count_launch(g->n_kernel_nodes);
+    return ABF_OK;
+    API_END
+}
+
+abf_status abf_batch_graph_kernels(const abf_batch_graph* g, uint32_t* n_out) {
+    if (!g || !n_out) return fail(ABF_ERR_INVALID, "null argument");
+    *n_out = g->n_kernel_nodes;
+    return ABF_OK;
+}
+
+abf_status abf_batch_graph_destroy(abf_batch_graph* g) {
+    API_BEGIN
+    if (!g) return ABF_OK;
+    cudaSetDevice(g->ix->device);
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+    return ABF_OK;
+    API_END
+}
+
 abf_status abf_query(abf_index* ix, const uint32_t* terms, uint32_t n_terms, abf_path path, uint32_t* d_bitmap,
                      uint32_t* d_ids, uint64_t ids_capacity, uint64_t* d_count, void* stream) {
     API_BEGIN

@@ -4,10 +4,12 @@ A batch of up to ``max_queries`` queries (``max_terms`` terms in total) is
 answered by one replay of a CUDA graph that holds the whole of
 ``abf_batch_run``: planning, merge tiles, scatter, probe and (optionally)
 compaction -- about ten kernel and memset nodes, launched by the host as a
-single graph launch. The graph is captured once for a fixed batch size on
-fixed device buffers; each batch copies its terms/offsets (and per-query
-paths) into those buffers on the executor's stream and replays. Shorter
-batches are padded with empty queries, which cost one zeroed bitmap each.
+single graph launch. The graph is captured by the C ABI
+(``abf_batch_graph_create`` / ``abf_batch_graph_replay``), once for a fixed
+batch size on fixed device buffers; each batch copies its terms/offsets (and
+per-query paths) into those buffers on the executor's stream and replays.
+Shorter batches are padded with empty queries, which cost one zeroed bitmap
+each.
 
 The reference launches six kernels per query (or per batch of at most 32)
 from the host after a synchronous, allocating Prepare
@@ -15,9 +17,12 @@ from the host after a synchronous, allocating Prepare
 """
 from __future__ import annotations
 
+import ctypes as C
+
 import numpy as np
 
 from . import _native as N
+from ._native import check, lib, ptr, stream_ptr
 
 
 class GraphBatchExecutor:
@@ -42,26 +47,24 @@ class GraphBatchExecutor:
         self.ws = index.workspace(self.max_q, self.max_t)
         self.stream = torch.cuda.Stream(device=dev)
         self.graph = None
+        self.kernel_nodes = 0
         self._n_set = 0
-
-    def _run_direct(self):
-        self.ix.batch_run(self.ws, self.d_terms, self.d_off, self.max_q, self.bitmaps, self.stride, path=self.path,
-                          d_paths=self.d_paths, d_ids=self.d_ids, d_id_offsets=self.d_id_off, stream=self.stream)
+        # the batch the graph is captured from: the offsets start as all-empty
+        # queries, a valid batch for the run that precedes the capture
+        self._batch = N.Batch(ptr(self.d_terms), ptr(self.d_off), self.max_q, ptr(self.d_paths), int(path),
+                              ptr(self.bitmaps), self.stride, ptr(self.d_ids),
+                              0 if self.d_ids is None else self.d_ids.numel(), ptr(self.d_id_off))
 
     def capture(self):
-        """Warm up once (module loading, attributes) and capture the graph."""
-        torch = self.torch
-        was = getattr(self.ix, "_profiling", False)
-        self.ix.profile(False)  # no event records inside the graph
-        with torch.cuda.stream(self.stream):
-            self._run_direct()
+        """Runs the batch once and captures it into a graph (abf_batch_graph_create)."""
+        h = C.c_void_p()
+        check(lib().abf_batch_graph_create(self.ix.handle, self.ws.handle, C.byref(self._batch),
+                                           stream_ptr(self.stream), C.byref(h)))
+        self.graph = h
+        n = C.c_uint32()
+        check(lib().abf_batch_graph_kernels(h, C.byref(n)))
+        self.kernel_nodes = int(n.value)
         self.stream.synchronize()
-        g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g, stream=self.stream):
-            self._run_direct()
-        self.graph = g
-        if was:
-            self.ix.profile(True)
         return self
 
     def set_batch(self, q_off: np.ndarray, q_terms: np.ndarray, paths: np.ndarray | None = None):
@@ -96,9 +99,19 @@ class GraphBatchExecutor:
         """Launches the graph on the executor's stream (after set_batch's copies)."""
         if self.graph is None:
             self.capture()
-        with self.torch.cuda.stream(self.stream):
-            self.graph.replay()
+        check(lib().abf_batch_graph_replay(self.graph, stream_ptr(self.stream)))
         return self
 
     def synchronize(self):
         self.stream.synchronize()
+
+    def free(self):
+        if self.graph is not None:
+            lib().abf_batch_graph_destroy(self.graph)
+            self.graph = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

@@ -312,6 +312,29 @@ typedef struct abf_batch {
 abf_status abf_batch_run(abf_index* index, abf_workspace* ws, const abf_batch* batch,
                          void* stream);
 
+/* A batch as one CUDA-graph launch. abf_batch_graph_create runs the batch
+ * once on `stream` (it must be a created stream, not the legacy default),
+ * then captures a second run into a CUDA graph and instantiates it: every
+ * kernel and memset node of abf_batch_run (planner, plan, queue scan, probe
+ * bits, dense group, merge tiles, scatter, probe, compaction). The graph
+ * keeps the device pointers and the query count of *batch: each
+ * abf_batch_graph_replay answers whatever terms, offsets and paths those
+ * arrays hold when it runs, so a caller refills them on the stream and
+ * replays (a shorter batch pads its offsets with empty queries). The index,
+ * the workspace and the batch's arrays must outlive the graph, and a
+ * workspace serves one graph or batch at a time. The arrays must hold a
+ * valid batch at creation (the first run reads them). The reference
+ * launches six kernels per query or per batch of at most 32 from the host
+ * (src/AdaBool/inverted_list.cu.h:185-228, test/adsfilter_batch.cu:453-502);
+ * this has no counterpart there. */
+typedef struct abf_batch_graph abf_batch_graph;
+abf_status abf_batch_graph_create(abf_index* index, abf_workspace* ws, const abf_batch* batch,
+                                  void* stream, abf_batch_graph** out);
+abf_status abf_batch_graph_replay(abf_batch_graph* graph, void* stream);
+/* Kernel nodes in the graph (the launches one replay makes). */
+abf_status abf_batch_graph_kernels(const abf_batch_graph* graph, uint32_t* n_out);
+abf_status abf_batch_graph_destroy(abf_batch_graph* graph);
+
 /* One query from host terms: bitmap (overwritten, (n_ads+31)/32 words) and,
  * if d_ids is not NULL, its ascending ids with the count in *d_count. Uses
  * the index's own workspace; the call returns after the terms were
