@@ -224,6 +224,10 @@ void default_tuning(abf_index* ix) {
     t.probe_min_fraction = 0.5f;
     t.group_min_queries = 32;
     t.fixed_tile_shape = 0;
+    // the reference keeps a 256-id bucket as a bitset from 33 ids on
+    // (src/AdaBool/inverted_list.h:425-458): a list of that density is
+    // merged per tile by the fixed rule
+    t.fixed_hybrid_min_len = uint32_t((33ull * ix->n_ads + 255) / 256);
 }
 
 void free_device(abf_index* ix) {
@@ -436,6 +440,7 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
     pa.path_uniform = uint32_t(b->path);
     pa.hybrid_min = t.heavy_min_len;
     pa.probe_min_frac = t.probe_min_fraction;
+    pa.fixed_hybrid_min = t.fixed_hybrid_min_len;
     pa.heavy_min = ws->heavy;
     pa.term_lpref = ws->lpref;
     pa.q_light_cnt = ws->lcnt;

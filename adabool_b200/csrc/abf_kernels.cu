@@ -248,7 +248,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 __global__ void __launch_bounds__(256) plan_kernel(IndexView ix, PlanArgs a) {
     __shared__ uint32_t s_warp[32];
     __shared__ unsigned long long s_red[8];
-    __shared__ uint32_t s_path;
+    __shared__ uint32_t s_path, s_max;
     __shared__ uint32_t s_mask[2048];  // the query's dense bitmaps (n_dense <= 65535)
     const uint32_t tid = threadIdx.x;
     for (uint32_t q = blockIdx.x; q < a.n_q; q += gridDim.x) {
@@ -261,14 +261,26 @@ __global__ void __launch_bounds__(256) plan_kernel(IndexView ix, PlanArgs a) {
         uint32_t path = a.paths ? a.paths[q] : a.path_uniform;
         if (path == ABF_PATH_AUTO) {
             // fixed rule: probe when the query's lists cover more than
-            // probe_min_frac of all blocks
+            // probe_min_frac of all blocks; else HYBRID when one of its lists
+            // has at least fixed_hybrid_min postings; else list-union
             uint64_t nb = 0;
+            uint32_t mx = 0;
             for (uint64_t i = qb + tid; i < qe; i += 256) {
                 const uint32_t t = a.terms[i];
-                if (t < ix.n_terms) nb += __ldg(ix.term_blk + t + 1) - __ldg(ix.term_blk + t);
+                if (t < ix.n_terms) {
+                    nb += __ldg(ix.term_blk + t + 1) - __ldg(ix.term_blk + t);
+                    mx = max(mx, __ldg(ix.term_len + t));
+                }
             }
-            nb = block_sum_u64<256>(nb, s_red);
-            path = (double(nb) > double(a.probe_min_frac) * double(ix.n_blocks)) ? ABF_PATH_PROBE : ABF_PATH_UNION;
+            if (tid == 0) s_max = 0;
+            nb = block_sum_u64<256>(nb, s_red);  // its barriers also order the s_max reset
+            mx = __reduce_max_sync(kFull, mx);
+            if (lane_id() == 0 && mx) atomicMax(&s_max, mx);
+            __syncthreads();
+            mx = s_max;
+            path = (double(nb) > double(a.probe_min_frac) * double(ix.n_blocks)) ? ABF_PATH_PROBE
+                   : (a.fixed_hybrid_min && mx >= a.fixed_hybrid_min) ? ABF_PATH_HYBRID
+                                                                      : ABF_PATH_UNION;
         }
         if (tid == 0) {
             if (path == ABF_PATH_PROBE) {

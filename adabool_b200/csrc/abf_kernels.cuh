@@ -52,6 +52,8 @@ struct PlanArgs {
     uint32_t path_uniform;    // abf_path when paths is null
     uint32_t hybrid_min;      // HYBRID merge threshold (postings)
     float probe_min_frac;     // fixed rule: probe when touched blocks / all blocks > this
+    uint32_t fixed_hybrid_min;  // fixed rule otherwise: HYBRID when a list has >= this many
+                                // postings (0: never), else UNION
     uint32_t* heavy_min;      // out: per query
     uint32_t* term_lpref;     // out: per term slot, exclusive prefix of scattered blocks
     uint64_t* q_light_cnt;    // out: per query scattered blocks

@@ -66,7 +66,11 @@ def _time_replays(ex, reps):
 
 
 def planner_experiment(n_train: int = 66_667, batch_config: str = "c2", reps: int = 3, device: int = 0,
-                       per_query_sample: int = 2048, verbose: bool = False) -> dict:
+                       per_query_sample: int = 2048, fixed_tau=None, verbose: bool = False) -> dict:
+    """fixed_tau: the fixed rule's probe threshold (from the reference
+    kernels' crossover, measured by the caller), or a callable
+    (index, q_off, q_terms, frac) -> dict with "tau" run on the evaluation
+    batch; None calibrates it on this library's own timing labels."""
     import torch
     t_start = time.time()
     cfg = W.CONFIGS[batch_config]
@@ -95,17 +99,24 @@ def planner_experiment(n_train: int = 66_667, batch_config: str = "c2", reps: in
     tr = P.train(Xtr, np.log(t_lab), epochs=120, batch=8192, lr=2e-3, device=device, verbose=verbose)
     train_s = time.time() - t0
     frac_tr = P.touched_fraction(ix, tqoff, tqt)
-    tau = P.calibrate_tau(frac_tr, t_lab)
+    tau_labels = P.calibrate_tau(frac_tr, t_lab)
     # --- evaluation batch ---
     qoff, qt = W.gen_queries(cfg.queries, lens)
     n = qoff.size - 1
+    tau_info = {"source": "this library's timing labels", "tau": tau_labels}
+    if callable(fixed_tau):
+        tau_info = dict(fixed_tau(ix, qoff, qt, P.touched_fraction(ix, qoff, qt)),
+                        source="crossover of the reference's kernels")
+    elif fixed_tau is not None:
+        tau_info = {"source": "given", "tau": float(fixed_tau)}
+    tau = float(tau_info.get("tau", tau_labels))
+    hyb_min = int(ix.tuning.fixed_hybrid_min_len)
     e_iso = P.collect_labels(ix, qoff, qt, device=device)
     e_lab = P.collect_labels_batched(ix, qoff, qt, e_iso, group=B, device=device)
     torch.cuda.empty_cache()
     Xev = _chunked_features(ix, qoff, qt, B, device)
     choice_pl = P.mlp_predict(tr.params, Xev, device).argmin(1)
-    frac = P.touched_fraction(ix, qoff, qt)
-    choice_fx = np.where(frac > tau, 0, 1)
+    choice_fx = P.fixed_rule_choice(ix, qoff, qt, tau, hyb_min)
     regret = {"planner": P.evaluate(e_lab, choice_pl), "fixed_rule": P.evaluate(e_lab, choice_fx),
               "always_probe": P.evaluate(e_lab, np.zeros(n, int)), "always_union": P.evaluate(e_lab, np.ones(n, int)),
               "always_hybrid": P.evaluate(e_lab, np.full(n, 2)),
@@ -174,7 +185,10 @@ def planner_experiment(n_train: int = 66_667, batch_config: str = "c2", reps: in
         "train": {"queries": n_train, "samples": int(t_lab.size), "label_seconds": round(label_s, 1),
                   "train_seconds": round(train_s, 1), "train_mse": tr.train_loss, "val_mse": tr.val_loss,
                   "epochs": tr.epochs},
-        "fixed_rule_tau": tau, "regret": regret, "batch": batch, "per_query_fixed": per_query,
+        "fixed_rule": {"tau": tau, "hybrid_min_len": hyb_min, "tau_from": tau_info, "tau_from_labels": tau_labels},
+        "regret": regret, "batch": batch, "per_query_fixed": per_query,
+        "speedup_planner_over_always_hybrid_batch":
+            batch["planner"]["queries_per_s"] / batch["always_hybrid"]["queries_per_s"],
         "speedup_planner_batch_over_per_query_fixed": batch["planner"]["queries_per_s"] / per_query["queries_per_s"],
         "speedup_planner_over_fixed_rule_batch": batch["planner"]["queries_per_s"] / batch["fixed_rule"]["queries_per_s"],
         "bitmap_mismatches_across_choices": mism,

@@ -9,7 +9,10 @@ cheapest (include/adabool.h, abf_planner_*). Here:
   train           fits the MLP with the library's own forward/backward and
                   Adam kernels (abf_mlp_grad / abf_mlp_adam), MSE on log us
   fixed_rule      the fallback: probe when the query's lists cover more than
-                  tau of all blocks, else list-union; tau calibrated on labels
+                  tau of all blocks, else HYBRID when one of its lists is as
+                  dense as a bucket the reference stores as a bitset, else
+                  list-union; tau from the crossover of the reference's own
+                  kernels (measured on the oracle side) or from labels
   evaluate        regret against the per-query best path
 
 Results are bit-exact whatever path is chosen; only time changes. The
@@ -238,6 +241,26 @@ def touched_fraction(index, q_off: np.ndarray, q_terms: np.ndarray) -> np.ndarra
     s = np.add.reduceat(b, q_off[:-1].astype(np.int64)) if q_terms.size else np.zeros(q_off.size - 1)
     s = np.where(np.diff(q_off) == 0, 0, s)
     return s / total
+
+
+def max_list_len(index, q_off: np.ndarray, q_terms: np.ndarray) -> np.ndarray:
+    """Longest list of each query (0 for an empty one)."""
+    lens = index.list_lengths().astype(np.int64)
+    valid = q_terms < index.n_terms
+    m = np.where(valid, lens[np.minimum(q_terms, index.n_terms - 1)], 0)
+    out = np.maximum.reduceat(m, q_off[:-1].astype(np.int64)) if q_terms.size else np.zeros(q_off.size - 1)
+    return np.where(np.diff(q_off) == 0, 0, out)
+
+
+def fixed_rule_choice(index, q_off: np.ndarray, q_terms: np.ndarray, tau: float, hybrid_min: int) -> np.ndarray:
+    """Output index (0 PROBE, 1 UNION, 2 HYBRID) the fixed rule of the plan
+    kernel picks: PROBE when the query's lists hold more than tau of all
+    blocks, else HYBRID when one of them has at least hybrid_min postings
+    (0: never), else UNION."""
+    frac = touched_fraction(index, q_off, q_terms)
+    mx = max_list_len(index, q_off, q_terms)
+    hyb = (mx >= hybrid_min) if hybrid_min else np.zeros(mx.shape, bool)
+    return np.where(frac > tau, 0, np.where(hyb, 2, 1))
 
 
 def calibrate_tau(frac: np.ndarray, times: np.ndarray) -> float:

@@ -615,10 +615,20 @@ def main():
     if args.mode == "planner" and args.impl == "ours":
         from adabool_b200 import experiments as X
         from adabool_b200 import planner as P
-        r = X.planner_experiment(n_train=args.train_queries, verbose=True)
+        from adabool_b200 import workload as W
+
+        def ref_tau(ix, qoff, qt, frac):
+            # the fixed rule's threshold: crossover of the reference's own
+            # kernels on the same index (oracle/ref_tau.py)
+            from oracle import ref_tau as RT
+            L = W.CONFIGS["c2"].lists
+            off, ads = W.gen_lists(L)
+            return RT.reference_tau(off, ads, L.n_terms, L.n_ads, qoff, qt, frac)
+
+        r = X.planner_experiment(n_train=args.train_queries, fixed_tau=ref_tau, verbose=True)
         params = r.pop("params")
         if args.planner_out:
-            P.save(params, args.planner_out, {k: r[k] for k in ("fixed_rule_tau", "tuning", "train")})
+            P.save(params, args.planner_out, {k: r[k] for k in ("fixed_rule", "tuning", "train")})
         r["metric"] = METRIC
         line = json.dumps(r)
         print(line, flush=True)

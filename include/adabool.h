@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define ABF_ABI_VERSION 1u
+#define ABF_ABI_VERSION 2u
 /* postings per compressed block of the list format */
 #define ABF_BLOCK_POSTINGS 128u
 
@@ -149,7 +149,7 @@ typedef struct abf_tuning {
     uint32_t probe_cap;       /* queries of one batch that may take the probe path (<= 65536) */
     float probe_min_fraction; /* fixed rule (ABF_PATH_AUTO without a planner): probe
                                  when the query's lists hold more than this fraction
-                                 of all blocks, else list-union */
+                                 of all blocks, else HYBRID or list-union (below) */
     uint32_t group_min_queries; /* batches of at least this many queries merge the
                                  dense bitmaps of all their dense-only queries in one
                                  pass per 64- or 32-word tile (each tile's slice of every
@@ -160,6 +160,12 @@ typedef struct abf_tuning {
                                  warps_per_tile runs the merge kernel with 8-warp CTAs
                                  and tiles narrowed down to 1,024 words; 1: always the
                                  given shape */
+    uint32_t fixed_hybrid_min_len; /* fixed rule: a query that does not probe takes HYBRID
+                                 when one of its lists has at least this many postings,
+                                 else list-union; 0 = never HYBRID. Default
+                                 ceil(33 * n_ads / 256): the density at which the
+                                 reference stores a 256-id bucket as a bitset
+                                 (src/AdaBool/inverted_list.h:425-458) */
 } abf_tuning;
 
 abf_status abf_get_tuning(const abf_index* index, abf_tuning* out);

@@ -32,7 +32,7 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
     # and the Python binding knows every one of them
     assert not (names - set(N.PROTOTYPES)), names - set(N.PROTOTYPES)
-    assert lib.abf_abi_version() == 1
+    assert lib.abf_abi_version() == 2
 
 
 def rand_lists(rng, n_terms, n_ads, max_len):
