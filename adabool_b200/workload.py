@@ -21,7 +21,43 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _native as N
-from ._native import check, lib, ptr
+from ._native import lib, ptr
+
+_GEN_FUNCS = ("abf_gen_target_lengths", "abf_gen_lists_offsets", "abf_gen_lists_fill", "abf_gen_queries_offsets",
+              "abf_gen_queries_fill")
+_gen = None       # library the generators run from (None: libadabool.so)
+_gen_err = None   # its last-error function
+
+
+def use_generator_library(L, last_error: str = "abf_last_error_string"):
+    """Runs the generators from the ctypes library L instead of libadabool.so
+    (L exports the abf_gen_* functions of include/abf_workload.h, e.g. a
+    standalone build of the same generator source); None restores the
+    default. The data are the same: the generator is a pure function of its
+    parameters."""
+    global _gen, _gen_err
+    if L is None:
+        _gen = _gen_err = None
+        return
+    for name in _GEN_FUNCS:
+        fn = getattr(L, name)
+        fn.argtypes = N.PROTOTYPES[name]
+        fn.restype = C.c_int
+    err = getattr(L, last_error)
+    err.argtypes = []
+    err.restype = C.c_char_p
+    _gen, _gen_err = L, err
+
+
+def _g():
+    return _gen if _gen is not None else lib()
+
+
+def check(status: int):
+    if status != N.ABF_OK:
+        msg = (_gen_err() if _gen_err is not None else lib().abf_last_error_string()).decode(errors="replace")
+        raise N.AbfError(status, msg)
+    return status
 
 
 @dataclass
@@ -84,16 +120,16 @@ def gen_lists(s: ListsSpec, n_threads: int = 0):
     """CSR (offsets uint64[n_terms+1], ads uint32[nnz]) of the synthetic filter matrix."""
     p = _lp(s, n_threads)
     off = np.empty(s.n_terms + 1, dtype=np.uint64)
-    check(lib().abf_gen_lists_offsets(C.byref(p), ptr(off, N.u64p)))
+    check(_g().abf_gen_lists_offsets(C.byref(p), ptr(off, N.u64p)))
     ads = np.empty(int(off[-1]), dtype=np.uint32)
-    check(lib().abf_gen_lists_fill(C.byref(p), ptr(off, N.u64p), ptr(ads, N.u32p)))
+    check(_g().abf_gen_lists_fill(C.byref(p), ptr(off, N.u64p), ptr(ads, N.u32p)))
     return off, ads
 
 
 def target_lengths(s: ListsSpec) -> np.ndarray:
     p = _lp(s, 0)
     out = np.empty(s.n_terms, dtype=np.uint32)
-    check(lib().abf_gen_target_lengths(C.byref(p), ptr(out, N.u32p)))
+    check(_g().abf_gen_target_lengths(C.byref(p), ptr(out, N.u32p)))
     return out
 
 
@@ -103,9 +139,9 @@ def gen_queries(q: QueriesSpec, list_len: np.ndarray, n_threads: int = 0):
     p = N.GenQueriesParams(q.n_queries, kind, q.median, q.sigma, q.lo, q.hi, q.seed, n_threads)
     ll = np.ascontiguousarray(list_len, dtype=np.uint32)
     off = np.empty(q.n_queries + 1, dtype=np.uint64)
-    check(lib().abf_gen_queries_offsets(C.byref(p), ptr(ll, N.u32p), ll.size, ptr(off, N.u64p)))
+    check(_g().abf_gen_queries_offsets(C.byref(p), ptr(ll, N.u32p), ll.size, ptr(off, N.u64p)))
     terms = np.empty(int(off[-1]), dtype=np.uint32)
-    check(lib().abf_gen_queries_fill(C.byref(p), ptr(ll, N.u32p), ll.size, ptr(off, N.u64p), ptr(terms, N.u32p)))
+    check(_g().abf_gen_queries_fill(C.byref(p), ptr(ll, N.u32p), ll.size, ptr(off, N.u64p), ptr(terms, N.u32p)))
     return off, terms
 
 

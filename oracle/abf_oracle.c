@@ -131,6 +131,7 @@ typedef struct {
     const uint32_t* q_terms;
     uint32_t n_queries;
     uint64_t* counts;
+    uint64_t* sums; /* optional: 2 per query (see orc_cpu_batch_sums) */
     uint64_t next; /* shared query cursor */
     pthread_mutex_t mu;
     uint64_t buf_cap;
@@ -145,8 +146,18 @@ static void* batch_worker(void* arg) {
         pthread_mutex_unlock(&j->mu);
         if (q >= j->n_queries) break;
         uint64_t b = j->q_off[q], e = j->q_off[q + 1];
-        j->counts[q] = orc_kway_union(j->offsets, j->ads, j->n_terms, j->q_terms + b, (uint32_t)(e - b), buf,
-                                      j->buf_cap);
+        uint64_t n = orc_kway_union(j->offsets, j->ads, j->n_terms, j->q_terms + b, (uint32_t)(e - b), buf,
+                                    j->buf_cap);
+        j->counts[q] = n;
+        if (j->sums) {
+            uint64_t s1 = 0, s2 = 0;
+            for (uint64_t i = 0; i < n && i < j->buf_cap; ++i) {
+                s1 += buf[i];
+                s2 += (uint64_t)buf[i] * i;
+            }
+            j->sums[2 * q] = s1;
+            j->sums[2 * q + 1] = s2;
+        }
     }
     free(buf);
     return NULL;
@@ -154,6 +165,12 @@ static void* batch_worker(void* arg) {
 
 uint64_t orc_cpu_batch(const uint64_t* offsets, const uint32_t* ads, uint32_t n_terms, const uint64_t* q_off,
                        const uint32_t* q_terms, uint32_t n_queries, int n_threads, uint64_t* counts) {
+    return orc_cpu_batch_sums(offsets, ads, n_terms, q_off, q_terms, n_queries, n_threads, counts, NULL);
+}
+
+uint64_t orc_cpu_batch_sums(const uint64_t* offsets, const uint32_t* ads, uint32_t n_terms, const uint64_t* q_off,
+                            const uint32_t* q_terms, uint32_t n_queries, int n_threads, uint64_t* counts,
+                            uint64_t* sums) {
     batch_job j;
     j.offsets = offsets;
     j.ads = ads;
@@ -162,6 +179,7 @@ uint64_t orc_cpu_batch(const uint64_t* offsets, const uint32_t* ads, uint32_t n_
     j.q_terms = q_terms;
     j.n_queries = n_queries;
     j.counts = counts;
+    j.sums = sums;
     j.next = 0;
     j.buf_cap = 0;
     /* the match set is written out (sorted ids), bounded by the sum of the

@@ -52,6 +52,12 @@ uint64_t orc_collect_ids(const uint8_t* bitmap, uint64_t bitmap_bytes, uint64_t 
  * threads; counts[q] gets each query's match count. Returns the total. */
 uint64_t orc_cpu_batch(const uint64_t* offsets, const uint32_t* ads, uint32_t n_terms, const uint64_t* q_off,
                        const uint32_t* q_terms, uint32_t n_queries, int n_threads, uint64_t* counts);
+/* The same, also writing two checksums of each query's ascending id list
+ * ids[0..n): sums[2q] = sum of ids[i], sums[2q+1] = sum of ids[i] * i, both
+ * mod 2^64 (the second depends on the order). */
+uint64_t orc_cpu_batch_sums(const uint64_t* offsets, const uint32_t* ads, uint32_t n_terms, const uint64_t* q_off,
+                            const uint32_t* q_terms, uint32_t n_queries, int n_threads, uint64_t* counts,
+                            uint64_t* sums);
 
 /* ---------------- the reference's mixed-container index ---------------- */
 enum { ORC_ARRAY1 = 0, ORC_ARRAY4, ORC_ARRAY8, ORC_ARRAY16, ORC_ARRAY32, ORC_BITSET, ORC_NTYPES };

@@ -2,6 +2,11 @@
 
   oracle/liborc.so               abf_oracle.c (gcc): k-way merge, mixed-format
                                  restatement, CPU baseline
+  oracle/libwgen.so              the seeded workload generator
+                                 (adabool_b200/csrc/abf_gen.cpp + gen_shim.cpp,
+                                 g++), so that the reference's timing leg
+                                 generates the benchmark data without loading
+                                 the product library
   oracle/_ref/libref_build.so    the reference's own ivf_list::BuildFrom,
                                  compiled with g++ from the reference sources
                                  (host memory only, no GPU needed)
@@ -10,9 +15,10 @@
                                  nvcc for sm_100a from the reference sources
 
 The two _ref libraries are built only where the reference source tree is
-present (REFERENCE_ROOT, default /root/reference); it is read in place and
-nothing is copied from it. The reference headers miss <array>/<memory>
-includes, which are added with -include.
+present: REFERENCE_ROOT if set, else a checkout named `reference` beside
+this repository's directory. It is read in place and nothing is copied from
+it. The reference headers miss <array>/<memory> includes, which are added
+with -include.
 """
 from __future__ import annotations
 
@@ -24,9 +30,10 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 REF_OUT = HERE / "_ref"
 LIBORC = HERE / "liborc.so"
+LIBWGEN = HERE / "libwgen.so"
 REF_BUILD = REF_OUT / "libref_build.so"
 REF_HARNESS = REF_OUT / "libref_harness.so"
-REFERENCE_ROOT = Path(os.environ.get("REFERENCE_ROOT", "/root/reference"))
+REFERENCE_ROOT = Path(os.environ.get("REFERENCE_ROOT") or HERE.parent.parent / "reference")
 SHIM = ["-include", "array", "-include", "memory"]
 
 
@@ -47,6 +54,16 @@ def build_orc() -> Path:
         _run(["gcc", "-O2", "-std=c99", "-fPIC", "-shared", "-Wall", "-D_POSIX_C_SOURCE=200809L",
               str(HERE / "abf_oracle.c"), "-o", str(LIBORC), "-lpthread"])
     return LIBORC
+
+
+def build_wgen() -> Path:
+    csrc = HERE.parent / "adabool_b200" / "csrc"
+    srcs = [csrc / "abf_gen.cpp", HERE / "gen_shim.cpp", csrc / "abf_internal.h",
+            HERE.parent / "include" / "abf_workload.h", HERE.parent / "include" / "adabool.h"]
+    if _stale(LIBWGEN, srcs):
+        _run(["g++", "-O3", "-std=c++17", "-fPIC", "-shared", "-Wall", "-march=x86-64-v2", str(csrc / "abf_gen.cpp"),
+              str(HERE / "gen_shim.cpp"), "-o", str(LIBWGEN), "-lpthread"])
+    return LIBWGEN
 
 
 def reference_present() -> bool:
@@ -72,8 +89,9 @@ def build_ref(with_gpu: bool = True) -> list[Path]:
 
 def build_all(with_gpu: bool = True):
     build_orc()
+    build_wgen()
     return build_ref(with_gpu)
 
 
 if __name__ == "__main__":
-    print(build_orc(), build_ref(with_gpu="--no-gpu" not in sys.argv))
+    print(build_orc(), build_wgen(), build_ref(with_gpu="--no-gpu" not in sys.argv))

@@ -44,6 +44,8 @@ def orc():
         L.orc_collect_ids.restype = C.c_uint64
         L.orc_cpu_batch.argtypes = [u64p, u32p, C.c_uint32, u64p, u32p, C.c_uint32, C.c_int, u64p]
         L.orc_cpu_batch.restype = C.c_uint64
+        L.orc_cpu_batch_sums.argtypes = [u64p, u32p, C.c_uint32, u64p, u32p, C.c_uint32, C.c_int, u64p, u64p]
+        L.orc_cpu_batch_sums.restype = C.c_uint64
         L.orc_mixed_build_coo.argtypes = [u32p, u32p, C.c_uint64, C.c_int]
         L.orc_mixed_build_coo.restype = C.c_void_p
         L.orc_mixed_build_csr.argtypes = [u64p, u32p, C.c_uint32, C.c_int]
@@ -150,11 +152,27 @@ def collect_ids(words: np.ndarray, ncols: int) -> np.ndarray:
     return out[:n].copy()
 
 
-def cpu_batch(off, ads, q_off, q_terms, n_threads: int) -> np.ndarray:
+def cpu_batch(off, ads, q_off, q_terms, n_threads: int, sums: bool = False):
+    """Heap k-way merge of every query on n_threads host threads: per-query
+    id counts, and with sums=True also (sum of ids, sum of ids * position)
+    mod 2^64 per query (an order-sensitive checksum of the sorted ids)."""
     counts = np.zeros(q_off.size - 1, dtype=np.uint64)
-    orc().orc_cpu_batch(_p(off, u64p), _p(ads, u32p), off.size - 1, _p(q_off, u64p), _p(q_terms, u32p),
-                        q_off.size - 1, n_threads, _p(counts, u64p))
-    return counts
+    q_off = np.ascontiguousarray(q_off, dtype=np.uint64)
+    q_terms = np.ascontiguousarray(q_terms, dtype=np.uint32)
+    if not sums:
+        orc().orc_cpu_batch(_p(off, u64p), _p(ads, u32p), off.size - 1, _p(q_off, u64p), _p(q_terms, u32p),
+                            q_off.size - 1, n_threads, _p(counts, u64p))
+        return counts
+    s = np.zeros((q_off.size - 1, 2), dtype=np.uint64)
+    orc().orc_cpu_batch_sums(_p(off, u64p), _p(ads, u32p), off.size - 1, _p(q_off, u64p), _p(q_terms, u32p),
+                             q_off.size - 1, n_threads, _p(counts, u64p), _p(s, u64p))
+    return counts, s
+
+
+def gen_lib():
+    """The standalone build of the workload generator (oracle/libwgen.so)."""
+    B.build_wgen()
+    return C.CDLL(str(B.LIBWGEN))
 
 
 class Mixed:

@@ -121,3 +121,33 @@ def test_reference_builder_if_present():
     for ty in range(O.NTYPES):
         for f in O.FIELDS:
             assert np.array_equal(m1.array(ty, f), m2.array(ty, f)), (ty, f)
+
+
+def test_standalone_generator_matches_library():
+    """oracle/libwgen.so (the generator source built on its own, used by the
+    reference's timing leg) yields the same workload as libadabool.so."""
+    from adabool_b200 import workload as W
+    spec = W.ListsSpec(n_terms=700, n_ads=90_001, nnz=60_000, zipf_s=1.1, max_len=9_000, seed=5)
+    qs = W.QueriesSpec(50, "lognormal", 8.0, 1.5, 1, 100, seed=6)
+    off_a, ads_a = W.gen_lists(spec)
+    q_a = W.gen_queries(qs, np.diff(off_a).astype(np.uint32))
+    W.use_generator_library(O.gen_lib(), "wgen_last_error_string")
+    try:
+        off_b, ads_b = W.gen_lists(spec)
+        q_b = W.gen_queries(qs, np.diff(off_b).astype(np.uint32))
+    finally:
+        W.use_generator_library(None)
+    assert np.array_equal(off_a, off_b) and np.array_equal(ads_a, ads_b)
+    assert np.array_equal(q_a[0], q_b[0]) and np.array_equal(q_a[1], q_b[1])
+
+
+def test_cpu_batch_checksums():
+    from adabool_b200 import workload as W
+    spec = W.ListsSpec(n_terms=300, n_ads=50_000, nnz=40_000, zipf_s=1.1, max_len=5_000, seed=9)
+    off, ads = W.gen_lists(spec)
+    qoff, qt = W.gen_queries(W.QueriesSpec(20, "lognormal", 6.0, 1.5, 1, 60, seed=3), np.diff(off).astype(np.uint32))
+    counts, sums = O.cpu_batch(off, ads, qoff, qt, 3, sums=True)
+    for i in range(qoff.size - 1):
+        e = O.kway_union(off, ads, qt[qoff[i]:qoff[i + 1]]).astype(np.uint64)
+        assert counts[i] == e.size
+        assert sums[i, 0] == e.sum() and sums[i, 1] == (e * np.arange(e.size, dtype=np.uint64)).sum()
