@@ -18,8 +18,13 @@ API in sub-batches. Inputs are larger than L2 (the compressed index alone is
          back device->host inside the timed region
   roofline / kernels
          per-kernel CUDA-event durations from the same steps run once more
-         on a single stream (no overlap), against the algorithmic bytes of
-         each kernel
+         on a single stream (no overlap), against the bytes each kernel's
+         design must move (dense bitmaps once per group-kernel launch, list
+         blocks, bitmap writes and reads, 4 bytes per id)
+  parity the untimed pass's ids of the first 256 queries against the CPU
+         oracle run of the cpu_baseline leg (count + two checksums per query)
+  reference_gpu
+         the reference's own CUDA kernels on the same index and queries
 
 Multi-GPU: replicas (each rank its own query set on its own copy of the
 index, no collective on the data path), launched by torchrun; the time is
@@ -27,7 +32,8 @@ the max over ranks.
 
 `--impl reference` times the reference's own CPU path (ComputeGroundTruth,
 test/adsfilter_q_all.cu:196-208, built from the reference sources into
-oracle/_ref) on the host cores, on a bounded sample of the same workload.
+oracle/_ref) on the host cores, on a bounded sample of the same workload
+(see run_reference).
 """
 from __future__ import annotations
 
@@ -49,8 +55,9 @@ sys.path.insert(0, str(ROOT))
 METRIC = "batched queries/s & postings GB/s vs HBM peak; learned vs fixed path planner"
 # dram__bytes_read.sum + dram__bytes_write.sum of one launch divided by that
 # launch's algorithmic bytes, from an ncu capture of the same kernel on the
-# same workload at 1/4 scale (write_ids: 766.89 MB of 766.78 MB)
-TRAFFIC_PER_ALGORITHMIC_BYTE = {"compact_write": 1.0001}
+# same workload at 1/4 scale (profiles/)
+TRAFFIC_PER_ALGORITHMIC_BYTE: dict = {}
+TRAFFIC_SOURCE: dict = {}
 UNIT = "queries/s"
 
 
@@ -73,7 +80,8 @@ def parse():
     p.add_argument("--tuning-set", default="",
                    help="explicit knobs instead of tuning, e.g. dense_div=256,tile_words=16384,group_min_queries=32")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (and with it the parity check)")
+    p.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference's CUDA kernels")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--out", default="", help="also append the JSON line to this file")
     p.add_argument("--mode", default="step", choices=["step", "planner", "serve", "index"],
@@ -185,6 +193,31 @@ def split(qoff, qterms, sb):
     return out
 
 
+def workload_config(cfg, n_postings: int, n_q: int) -> dict:
+    """The `config` object of both arms' lines: the workload only (the
+    execution settings of our arm go to its `execution` key)."""
+    L, Q = cfg.lists, cfg.queries
+    return {"workload": f"{cfg.name}: {L.n_terms} terms x {L.n_ads} ads, {n_postings} postings "
+                        f"(Zipf {L.zipf_s:g} lengths clipped to [1, {L.max_len}], seed {L.seed}); {n_q} queries "
+                        f"({Q.kind} term counts, median {Q.median:g}, sigma {Q.sigma:g}, [{Q.lo}, {Q.hi}], seed {Q.seed})",
+            "output": "per query: bitmap over all ads + ascending uint32 ad ids",
+            "l2": "inputs larger than L2 (no flush)"}
+
+
+PARITY_QUERIES = 256  # queries whose ids get a checksum in the untimed pass
+
+
+def id_checksums(ids, n: int, torch):
+    """(sum of ids, sum of ids * position) mod 2^64 of an ascending id list on
+    the device, the same checksums as the oracle's orc_cpu_batch_sums."""
+    if n == 0:
+        return 0, 0
+    x = ids[:n].to(torch.int64) & 0xFFFFFFFF
+    s1 = int(x.sum().item()) & 0xFFFFFFFFFFFFFFFF
+    s2 = int((x * torch.arange(n, device=ids.device, dtype=torch.int64)).sum().item()) & 0xFFFFFFFFFFFFFFFF
+    return s1, s2
+
+
 def run_ours(args, rank, world, dev):
     import torch
     import adabool_b200 as ab
@@ -196,7 +229,6 @@ def run_ours(args, rank, world, dev):
     t0 = time.time()
     ix = Index.from_csr(off, ads, L.n_terms, L.n_ads, device=dev)
     build_s = time.time() - t0
-    st = ix.stats()
     n_q = qoff.size - 1
     n_words = (L.n_ads + 31) // 32
     stride = (n_words + 3) // 4 * 4
@@ -265,7 +297,10 @@ def run_ours(args, rank, world, dev):
             e.record(s)
             stream.wait_event(e)
 
-    # correctness spot check + result sizes (untimed)
+    # untimed pass: result sizes of every query and checksums of the first
+    # PARITY_QUERIES queries' ids (compared with the oracle in cpu_baseline)
+    n_par = min(PARITY_QUERIES, n_q)
+    sums = np.zeros((n_par, 2), np.uint64)
     with torch.cuda.stream(stream):
         counts = np.zeros(n_q, np.uint64)
         for (a, b, _, _), (dt, do, nq) in zip(sbs, d_in):
@@ -274,6 +309,8 @@ def run_ours(args, rank, world, dev):
             stream.synchronize()
             o = idoff[0][:nq + 1].cpu().numpy()
             counts[a:b] = np.diff(o)
+            for i in range(a, min(b, n_par)):
+                sums[i] = id_checksums(ids[0][int(o[i - a]):], int(o[i - a + 1] - o[i - a]), torch)
     ws[0].check(stream)
 
     for _ in range(args.warmup):
@@ -294,6 +331,8 @@ def run_ours(args, rank, world, dev):
     ms_total = e0.elapsed_time(e1)
     ms_step = dist_max(ms_total / args.steps, world)
     dist_barrier(world)
+    for w in ws:
+        w.check(stream)
 
     # per-kernel CUDA-event times for the roofline: the same K steps once
     # more on one stream, so no kernel's duration includes another's
@@ -308,59 +347,99 @@ def run_ours(args, rank, world, dev):
     kern = ix.profile_read()
     ix.profile(False)
 
+    # the same step without the id lists (bitmaps only, what the reference's
+    # kernels produce), device-timed, for the reference-kernel comparison
+    reps = max(1, args.steps // 2)
+    with torch.cuda.stream(stream):
+        def bm_step():
+            for (dt, do, nq) in d_in:
+                ix.batch_run(ws[0], dt, do, nq, bms[0], stride, path=path, stream=stream)
+        bm_step()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(reps):
+            bm_step()
+        f1.record(stream)
+        f1.synchronize()
+    bitmaps_only_qps = n_q / (f0.elapsed_time(f1) / reps / 1e3)
+
     # ---- e2e through the public API from pinned host buffers ----
     e2e = None
     if not args.no_e2e:
         e2e = run_e2e(args, ix, sbs, ws, bms, ids, idoff, stride, path, dev, world, n_q)
 
-    # ---- algorithmic bytes (roofline numerator) ----
-    # a list is read in the representation its kernel uses: the merge kernel
-    # reads a dense bitmap (n_ads/8 bytes) where the list has one, blocks
-    # (payload + 16 B metadata each) otherwise; the scatter kernel reads blocks
+    # ---- physical bytes per kernel (roofline numerators) ----
+    # every kernel is charged the bytes its design must move once: the dense
+    # group kernel reads each dense bitmap once per launch and writes the
+    # bitmaps of the queries it covers; the merge kernel reads the blocks of
+    # the merged lists that have no dense bitmap (and, with the group kernel
+    # on, reads back and rewrites the tiles of the queries that have such
+    # lists); the scatter kernel reads the blocks of the scattered lists and
+    # read-modify-writes one 4-byte word per posting; the compaction reads
+    # each bitmap once and writes 4 bytes per id
     bm_bytes = L.n_ads / 8.0
+    st = ix.stats()  # after tuning (the dense bitmaps follow dense_div)
     lbytes = ix.list_bytes().astype(np.float64)
     dense_t = (ix.list_flags() & 1) != 0
     hm = ix.tuning.heavy_min_len
     merged_t = {ab.PATH_HYBRID: dense_t | (lens >= hm), ab.PATH_TILE: np.ones_like(dense_t),
                 ab.PATH_UNION: dense_t, ab.PATH_AUTO: dense_t,
                 ab.PATH_PROBE: np.zeros_like(dense_t)}[path]
-    read_t = np.where(dense_t & merged_t, bm_bytes, lbytes)
     seg = qoff[:-1].astype(np.int64)
     empty = np.diff(qoff) == 0
 
     def per_query(x):
         if not qterms.size:
             return np.zeros(n_q)
-        return np.where(empty, 0.0, np.add.reduceat(x, seg))
+        return np.where(empty, 0.0, np.add.reduceat(x.astype(np.float64), seg))
 
-    q_merge = per_query(np.where(merged_t[qterms], read_t[qterms], 0.0))
-    q_all = per_query(read_t[qterms])
-    alg = {
-        "tile_union": float(np.sum(q_merge)) + n_q * bm_bytes,
-        "scatter_union": float(np.sum(q_all - q_merge)),
-        "compact_count": n_q * bm_bytes,
-        "compact_write": n_q * bm_bytes + 4.0 * float(counts.sum()),
-    }
-    if "dense_group" in kern:
-        # the group kernel reads every dense bitmap once per launch and writes
-        # the bitmaps of the queries whose merged lists are all dense; the
-        # merge kernel keeps the others
-        n_dense = int(dense_t.sum())
-        dense_only = (per_query((merged_t & ~dense_t)[qterms].astype(np.float64)) == 0) & ~empty
-        alg["dense_group"] = kern["dense_group"][0] / args.steps * n_dense * bm_bytes + \
-            float(dense_only.sum()) * bm_bytes
-        alg["tile_union"] = float(np.sum(q_merge[~dense_only])) + float((~dense_only).sum()) * bm_bytes
-    total_alg = float(np.sum(q_all)) + 16.0 * qterms.size + 2 * n_q * bm_bytes + 4.0 * float(counts.sum())
+    qt_m, qt_d = merged_t[qterms], dense_t[qterms]
+    q_merge_nd = per_query(np.where(qt_m & ~qt_d, lbytes[qterms], 0.0))       # merged from blocks
+    q_merge_nd_n = per_query((qt_m & ~qt_d).astype(np.float64))
+    q_dense_n = per_query((qt_m & qt_d).astype(np.float64))                   # merged dense lists
+    q_scat = per_query(np.where(~qt_m, lbytes[qterms], 0.0))
+    q_scat_post = per_query(np.where(~qt_m, lens[qterms], 0).astype(np.float64))
+    group_on = "dense_group" in kern
+    alg = {"scatter_union": float(q_scat.sum() + 8.0 * q_scat_post.sum()),
+           "compact": n_q * bm_bytes + 4.0 * float(counts.sum())}
+    dense_only = (q_merge_nd_n == 0) & ~empty
+    if group_on:
+        g_launches = kern["dense_group"][0] / args.steps
+        alg["dense_group"] = g_launches * float(st["dense_bytes"]) + float((~empty).sum()) * bm_bytes
+        alg["tile_union"] = float(q_merge_nd[~dense_only & ~empty].sum()) + \
+            2.0 * bm_bytes * float((~dense_only & ~empty).sum()) + bm_bytes * float(empty.sum())
+    else:
+        alg["tile_union"] = float(q_merge_nd.sum() + q_dense_n.sum() * bm_bytes) + n_q * bm_bytes
     hbm, peak_kind = peaks()
+    cs = clk.summary()
+    sm_mhz = (cs or {}).get("sm_mhz") or 1965.0
+    n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
+    smem_peak = n_sm * 128.0 * sm_mhz * 1e6 / 1e9  # GB/s: 128 bytes per clock per SM
     per_kernel = {}
+    total_ms = sum(v[1] for v in kern.values())
     for name, (nl, tms) in kern.items():
-        per_launch_ms = tms / max(nl, 1)
         d = {"launches_per_step": nl / args.steps, "ms_per_step": tms / args.steps,
-             "share": tms / max(sum(v[1] for v in kern.values()), 1e-9)}
+             "share": tms / max(total_ms, 1e-9)}
         if name in alg and tms > 0:
+            d["bytes_per_step"] = alg[name]
             d["achieved_gbs"] = alg[name] * args.steps / (tms / 1e3) / 1e9
             d["frac_of_" + peak_kind] = d["achieved_gbs"] / hbm
         per_kernel[name] = d
+    if group_on and kern["dense_group"][1] > 0:
+        # its bound is the shared-memory pipe: one 256-byte row load per
+        # (query, dense list, 64-word tile)
+        pairs = float(q_dense_n.sum())
+        g = per_kernel["dense_group"]
+        g["bound"] = "shared memory"
+        g["smem_gbs"] = pairs * bm_bytes * args.steps / (kern["dense_group"][1] / 1e3) / 1e9
+        g["smem_peak_gbs"] = round(smem_peak, 1)
+        g["frac_of_smem_peak"] = g["smem_gbs"] / smem_peak
+        g["query_dense_pairs_per_step"] = pairs
+    if "scatter_union" in per_kernel and kern["scatter_union"][1] > 0:
+        sc = per_kernel["scatter_union"]
+        sc["bound"] = "L2 atomics"
+        sc["postings_per_step"] = float(q_scat_post.sum())
+        sc["atomic_postings_per_s"] = float(q_scat_post.sum()) * args.steps / (kern["scatter_union"][1] / 1e3)
     dom = max(per_kernel, key=lambda k: per_kernel[k]["ms_per_step"]) if per_kernel else None
     roof = None
     if dom and "achieved_gbs" in per_kernel[dom]:
@@ -372,34 +451,35 @@ def run_ours(args, rank, world, dev):
         roof = {"kernel": dom, "bound": "hbm", "achieved": round(a, 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(a / hbm, 4), "peak_kind": peak_kind, "traffic": traffic,
                 "alg_bytes_per_launch": round(alg[dom] / n_launch),
-                "traffic_source": None if ratio is None else
-                "ncu capture of this kernel at 1/4 scale (profiles/), scaled by the ids a launch writes",
+                "traffic_source": None if ratio is None else TRAFFIC_SOURCE.get(dom),
                 "duration_source": "CUDA events around each launch in a single-stream pass of the same steps "
                                    "right after the timed region"}
+    step_bytes = float(sum(alg.values()))
     postings = float(np.sum(qpost))
     value = n_q * world / (ms_step / 1e3)
     res = {
         "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded Zipf lists, lognormal queries)",
-        "config": {"workload": f"{cfg.name}: {L.n_terms} terms x {L.n_ads} ads, {st['n_postings']} postings; "
-                               f"{n_q} queries/rank, sub-batches of {args.sub_batch} on {n_streams} streams",
-                   "path": args.path, "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (no flush)",
-                   "index_bytes": ix.stats()["device_bytes"],
-                   "tuning": dict(ix.tuning.as_dict(), dense_div=ix.dense_div), "autotune": tune_info},
+        "config": workload_config(cfg, int(st["n_postings"]), n_q),
+        "execution": {"path": args.path, "parallelism": f"replicas{world}",
+                      "sub_batch": args.sub_batch, "streams": n_streams, "index_bytes": st["device_bytes"],
+                      "tuning": dict(ix.tuning.as_dict(), dense_div=ix.dense_div), "autotune": tune_info},
         "postings_per_s": round(postings * world / (ms_step / 1e3), 1),
         "postings_raw_gbs": round(4 * postings * world / (ms_step / 1e3) / 1e9, 1),
-        "algorithmic_gbs": round(total_alg * world / (ms_step / 1e3) / 1e9, 1),
+        "algorithmic_gbs": round(step_bytes * world / (ms_step / 1e3) / 1e9, 1),
+        "algorithmic_bytes_per_step": round(step_bytes),
+        "bitmaps_only_qps": round(bitmaps_only_qps * world, 1),
         "roofline": roof, "kernels": per_kernel, "gpu_launches": int(launches),
         "result_ids_per_step": int(counts.sum()),
         "setup_s": {"generate": round(gen_s, 2), "build_upload": round(build_s, 2)},
     }
-    cs = clk.summary()
     if cs:
         res["clocks"] = cs
     if e2e:
         res["e2e"] = e2e
-    return res, (off, ads, qoff, qterms, counts)
+    return res, dict(off=off, ads=ads, qoff=qoff, qterms=qterms, counts=counts, sums=sums, ix=ix, cfg=cfg,
+                     dev=dev)
 
 
 def run_e2e(args, ix, sbs, ws, bms, ids, idoff, stride, path, dev, world, n_q):
@@ -460,12 +540,18 @@ def run_e2e(args, ix, sbs, ws, bms, ids, idoff, stride, path, dev, world, n_q):
     ms = dist_max(e0.elapsed_time(e1) / args.steps, world)
     return {"value": round(n_q * world / (ms / 1e3), 2), "unit": UNIT, "ms_per_step": round(ms, 3),
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-            "note": "query terms host->device and every sorted id list device->host, pinned buffers, 2 streams"}
+            "note": "query terms host->device and every sorted id list device->host, pinned buffers, 2 streams",
+            "bound": f"PCIe: the device->host copy of the id lists, {d2h / (ms / 1e3) / 1e9:.1f} GB/s; kernel work "
+                     "moves the device-timed value, not this one"}
 
 
-def cpu_baseline(off, ads, qoff, qterms, seconds: float):
-    """Oracle k-way merge (a port of the match-set semantics) on all host cores."""
+def cpu_baseline(data: dict, seconds: float):
+    """Oracle k-way merge (a port of the match-set semantics) on all host
+    cores, on a bounded sample of the same queries. Its results are also the
+    parity check of the untimed pass: per query the id count and two
+    checksums of the ascending ids must equal ours."""
     from oracle import oracle as O
+    off, ads, qoff, qterms = data["off"], data["ads"], data["qoff"], data["qterms"]
     n_threads = os.cpu_count() or 1
     lens = np.diff(off)
     # single-core rate on the first query with work
@@ -480,60 +566,212 @@ def cpu_baseline(off, ads, qoff, qterms, seconds: float):
     m = int(np.searchsorted(np.cumsum(qpost), budget)) + 1
     m = max(min(m, qoff.size - 1), min(n_threads, qoff.size - 1))
     t0 = time.time()
-    O.cpu_batch(off, ads, qoff[:m + 1], qterms[:qoff[m]], n_threads)
+    counts, sums = O.cpu_batch(off, ads, qoff[:m + 1], qterms[:qoff[m]], n_threads, sums=True)
     dt = time.time() - t0
+    # parity of our untimed pass against these oracle results
+    k = min(m, data["sums"].shape[0])
+    bad = [int(i) for i in range(k) if counts[i] != data["counts"][i] or
+           not np.array_equal(sums[i], data["sums"][i])]
+    parity = {"checked": k, "mismatches": len(bad), "first_mismatches": bad[:8],
+              "against": "oracle heap k-way merge (orc_kway_union): per query the id count, the sum of the ids "
+                         "and the sum of id x position (mod 2^64) of our ascending id list",
+              "queries": f"the first {k} queries of the step"}
     return {"value": round(m / dt, 3), "unit": UNIT, "cores": n_threads, "kind": "port",
             "sample": f"first {m} queries of the same set ({qpost[:m].sum():.3g} postings), heap k-way merge "
                       f"to sorted ids, {n_threads} threads, {dt:.1f} s",
-            "single_core_value": round(1.0 / one, 3), "single_core_sample": f"query {i0} ({post0:.3g} postings)"}
+            "single_core_value": round(1.0 / one, 3), "single_core_sample": f"query {i0} ({post0:.3g} postings)"}, \
+        parity
+
+
+def reference_gpu(data: dict, sample: int = 32) -> dict:
+    """The reference's own CUDA kernels (yxr620/AdaBool, compiled from its
+    sources for sm_100a into oracle/_ref/libref_harness.so) on the same
+    index and queries, beside ours. Its std::map builder cannot build 500M
+    postings in reasonable time, so its arrays come from the oracle's
+    restatement of that builder (pinned array for array against the real one
+    by tests/test_oracle.py); the reference then derives its block metadata
+    and runs its kernels unmodified. Per sampled query: Prepare(keys) +
+    ListUnion_sparse (test/adsfilter_q_all.cu:427-438) and Prepare(len, bm) +
+    ListUnion_dense (test/adsfilter_q_all.cu:414-425); one batch of 32
+    through RunArraysImpl<32> (the path of BatchListUnion_dense) and the six
+    RunSparseBatchListUnion launches of BatchListUnion_sparse
+    (test/adsfilter_batch.cu:28-79). Kernels timed with CUDA events, the
+    host Prepare with a host clock; every reference bitmap is compared with
+    ours. Bitmaps only: the reference has no id-list kernel."""
+    import ctypes as C
+    import torch
+    import adabool_b200 as ab
+    from oracle import oracle as O
+    H = O.ref_harness_lib()
+    if H is None:
+        return {"unavailable": "oracle/_ref/libref_harness.so was not built (needs the reference sources)"}
+    off, ads, qoff, qterms, ix, cfg = (data[k] for k in ("off", "ads", "qoff", "qterms", "ix", "cfg"))
+    L = cfg.lists
+    t0 = time.time()
+    mixed = O.Mixed.from_csr(off, ads)
+    arrs = {f: [mixed.array(t, f) for t in range(O.NTYPES)] for f in ("key_seg", "headers", "keys", "arrays")}
+    mixed.free()
+    mixed_s = time.time() - t0
+
+    def ptrs(lst, ct):
+        return (ct * O.NTYPES)(*[x.ctypes.data_as(ct) if x.size else C.cast(None, ct) for x in lst])
+
+    t0 = time.time()
+    h = H.refq_gpu_load(ptrs(arrs["key_seg"], O.u32p), (C.c_uint64 * O.NTYPES)(*[x.size for x in arrs["key_seg"]]),
+                        ptrs(arrs["headers"], O.u32p), (C.c_uint64 * O.NTYPES)(*[x.size for x in arrs["headers"]]),
+                        ptrs(arrs["keys"], O.u32p), ptrs(arrs["arrays"], O.u8p),
+                        (C.c_uint64 * O.NTYPES)(*[x.size for x in arrs["arrays"]]))
+    load_s = time.time() - t0
+    ref_bytes = int(sum(x.nbytes for v in arrs.values() for x in v))
+    del arrs
+    dev = data["dev"]
+    n_words = (L.n_ads + 31) // 32
+    stream = torch.cuda.current_stream(dev)
+    sp = C.c_void_p(stream.cuda_stream)
+    ours = torch.empty(n_words, dtype=torch.int32, device=dev)
+    ref = torch.zeros(n_words + 64, dtype=torch.int32, device=dev)
+    pm, km = C.c_float(), C.c_float()
+    sparse, dense, ours_ms = [], [], []
+    mismatches = 0
+    n = min(sample, qoff.size - 1)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    batch = {}
+    try:
+        for i in range(n):
+            q = np.ascontiguousarray(qterms[qoff[i]:qoff[i + 1]], dtype=np.uint32)
+            ix.query(q, ours, path=ab.PATH_HYBRID, stream=stream)  # warm
+            e0.record(stream)
+            ix.query(q, ours, path=ab.PATH_HYBRID, stream=stream)
+            e1.record(stream)
+            e1.synchronize()
+            ours_ms.append(e0.elapsed_time(e1))
+            want = ours.cpu().numpy()
+            ref.zero_()
+            rc = H.refq_gpu_sparse(h, q.ctypes.data_as(O.u32p), q.size, C.c_void_p(ref.data_ptr()), sp, C.byref(pm),
+                                   C.byref(km))
+            sparse.append((pm.value, km.value))
+            mismatches += int(rc != 0 or not np.array_equal(ref[:n_words].cpu().numpy(), want))
+            # padded so the reference's 16-byte bitmap reads stay inside the buffer
+            qb = np.concatenate([O.term_bitmap_bytes(q, L.n_terms, pad_to=16), np.zeros(32, np.uint8)])
+            ref.zero_()
+            rc = H.refq_gpu_dense(h, qb.ctypes.data_as(O.u8p), qb.size, C.c_void_p(ref.data_ptr()), sp, C.byref(pm),
+                                  C.byref(km))
+            dense.append((pm.value, km.value))
+            mismatches += int(rc != 0 or not np.array_equal(ref[:n_words].cpu().numpy(), want))
+        B = min(32, qoff.size - 1)
+        bqs = [np.ascontiguousarray(qterms[qoff[i]:qoff[i + 1]], dtype=np.uint32) for i in range(B)]
+        qlen = ((L.n_terms + 7) // 8 + 15) // 16 * 16 + 32
+        bm = np.zeros(B * qlen, np.uint8)
+        for i, q in enumerate(bqs):
+            b = O.term_bitmap_bytes(q, L.n_terms, pad_to=16)
+            bm[i * qlen:i * qlen + b.size] = b
+        res_len = (n_words + 3) // 4 * 4
+        dres = torch.zeros(B * res_len, dtype=torch.int32, device=dev)
+        got_d = None
+        if B == 32:
+            rc = H.refq_gpu_batch_dense32(h, bm.ctypes.data_as(O.u8p), qlen, C.c_void_p(dres.data_ptr()), res_len,
+                                          sp, C.byref(pm), C.byref(km))
+            batch["BatchListUnion_dense_b32"] = {"prep_ms": pm.value, "kernel_ms": km.value,
+                                                 "kernel_qps": round(32e3 / km.value, 1), "rc": int(rc)}
+            got_d = dres.cpu().numpy().reshape(B, res_len)
+        keys = np.concatenate(bqs).astype(np.uint32)
+        qidx = np.concatenate([np.full(q.size, i, np.uint32) for i, q in enumerate(bqs)])
+        dres.zero_()
+        rc = H.refq_gpu_batch_sparse(h, keys.ctypes.data_as(O.u32p), qidx.ctypes.data_as(O.u32p), keys.size,
+                                     C.c_void_p(dres.data_ptr()), res_len * 4, sp, C.byref(pm), C.byref(km))
+        batch[f"BatchListUnion_sparse_b{B}"] = {"prep_ms": pm.value, "kernel_ms": km.value,
+                                                "kernel_qps": round(B * 1e3 / km.value, 1), "rc": int(rc)}
+        got_s = dres.cpu().numpy().reshape(B, res_len)
+        for i, q in enumerate(bqs):
+            ix.query(q, ours, path=ab.PATH_HYBRID, stream=stream)
+            want = ours.cpu().numpy()
+            if got_d is not None:
+                mismatches += int(not np.array_equal(got_d[i, :n_words], want))
+            mismatches += int(not np.array_equal(got_s[i, :n_words], want))
+    finally:
+        H.refq_gpu_free(h)
+
+    def stats(v):
+        a = np.array(v)
+        return {"prep_ms_mean": round(float(a[:, 0].mean()), 4), "kernel_ms_mean": round(float(a[:, 1].mean()), 4),
+                "kernel_qps": round(float(1e3 / a[:, 1].mean()), 1),
+                "with_prep_qps": round(float(1e3 / (a[:, 0] + a[:, 1]).mean()), 1)}
+
+    return {"what": "reference CUDA kernels (built from its sources for sm_100a), bitmaps only, same index and "
+                    "queries", "sample_queries": n,
+            "ListUnion_sparse": stats(sparse), "ListUnion_dense": stats(dense), **batch,
+            "ours_per_query_qps": round(float(1e3 / np.mean(ours_ms)), 1),
+            "ours_per_query_note": "abf_query (HYBRID), one query per call, bitmap only, CUDA events",
+            "bitmap_mismatches_vs_ours": mismatches, "reference_index_bytes": ref_bytes,
+            "setup_s": {"mixed_build": round(mixed_s, 2), "reference_load": round(load_s, 2)}}
 
 
 # ---------------------------------------------------------------------------
+REF_COO_STRIDE = 16  # the reference arm scans every 16th COO pair and scales by 16
+
+
 def run_reference(args):
-    """The reference's CPU path on the host cores (bounded sample)."""
+    """The reference's CPU path on the host cores (bounded sample).
+
+    The reference computes a query's match set on the CPU with
+    ComputeGroundTruth (test/adsfilter_q_all.cu:196-208): one pass over every
+    (term, ad) pair of the filter matrix with a std::set lookup of the term,
+    inserting hits into a std::set of ads. It costs ~40 s per query at c1 on
+    one core, so each step is a bounded sample: as many queries as host
+    threads, one per thread, each scanning a 1/16 stride sample of the COO
+    pairs (every 16th pair, so hits keep their proportion); the step time is
+    scaled by 16 to a full scan. The workload comes from oracle/libwgen.so
+    (the same generator source as the product library, built on its own), so
+    this process loads no library of the product."""
     from oracle import oracle as O
     from adabool_b200 import workload as W
+    W.use_generator_library(O.gen_lib(), "wgen_last_error_string")
     cfg, off, ads, lens, qoff, qterms, _ = make_workload(args.config, args.scale, args.queries, 0)
+    n_q = qoff.size - 1
     n_threads = os.cpu_count() or 1
     H = O.ref_harness_lib()
-    qpost = np.array([lens[qterms[qoff[i]:qoff[i + 1]]].sum() for i in range(qoff.size - 1)], np.float64)
+    base = {"impl": "reference", "metric": METRIC, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded Zipf lists, lognormal queries)",
+            "config": workload_config(cfg, int(off[-1]), n_q)}
     if H is not None:
         terms, ads_c = W.lists_to_coo(off, ads)
-        h = H.refq_cpu_load(O._p(np.ascontiguousarray(terms), O.u32p), O._p(ads_c, O.u32p), terms.size)
-        kind = "reference"
-        desc = "ComputeGroundTruth (reference CPU path, std::set over every COO pair)"
+        ts = np.ascontiguousarray(terms[::REF_COO_STRIDE])
+        as_ = np.ascontiguousarray(ads_c[::REF_COO_STRIDE])
+        del terms, ads_c
+        h = H.refq_cpu_load(O._p(ts, O.u32p), O._p(as_, O.u32p), ts.size)
+        kind, scale = "reference", float(REF_COO_STRIDE)
+        desc = (f"ComputeGroundTruth (the reference's CPU path: a std::set lookup per COO pair) over every "
+                f"{REF_COO_STRIDE}th of the {int(off[-1])} COO pairs, time x{REF_COO_STRIDE}")
 
-        def run(m):
+        def run(q0, m):
             counts = np.zeros(m, np.uint64)
-            H.refq_ground_truth_batch(h, O._p(np.ascontiguousarray(qoff[:m + 1]), O.u64p),
-                                      O._p(np.ascontiguousarray(qterms[:qoff[m]]), O.u32p), m, n_threads,
-                                      O._p(counts, O.u64p))
+            qo = np.ascontiguousarray(qoff[q0:q0 + m + 1] - qoff[q0])
+            qt = np.ascontiguousarray(qterms[qoff[q0]:qoff[q0 + m]])
+            H.refq_ground_truth_batch(h, O._p(qo, O.u64p), O._p(qt, O.u32p), m, n_threads, O._p(counts, O.u64p))
     else:
-        kind = "port"
-        desc = "oracle heap k-way merge (reference library not built)"
+        kind, scale = "port", 1.0
+        desc = "oracle heap k-way merge (the reference library was not built)"
 
-        def run(m):
-            O.cpu_batch(off, ads, qoff[:m + 1], qterms[:qoff[m]], n_threads)
-    # the reference's scan costs the same per query whatever its size: one
-    # query per thread per step keeps a step to a few seconds
-    m = min(n_threads, qoff.size - 1) if kind == "reference" else max(1, min(qoff.size - 1, n_threads))
-    for _ in range(args.warmup):
-        run(min(m, n_threads))
+        def run(q0, m):
+            O.cpu_batch(off, ads, qoff[q0:q0 + m + 1] - qoff[q0], qterms[qoff[q0]:qoff[q0 + m]], n_threads)
+    m = max(1, min(n_threads, n_q))
+    nxt = 0
     times = []
-    for _ in range(args.steps):
+    for k in range(args.warmup + args.steps):
+        q0 = nxt if nxt + m <= n_q else 0
+        nxt = q0 + m
         t0 = time.time()
-        run(m)
-        times.append(time.time() - t0)
-    sec = float(np.mean(times))
+        run(q0, m)
+        if k >= args.warmup:
+            times.append(time.time() - t0)
+    sec = float(np.mean(times)) * scale  # per step of m queries over the full COO
     v = m / sec
-    sample = f"{desc}: first {m} queries of {cfg.name} per step ({qpost[:m].sum():.3g} postings), {n_threads} threads"
-    return {"impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(sec * 1e3, 1), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": f"{cfg.name}: {cfg.lists.n_terms} terms x {cfg.lists.n_ads} ads, "
-                                   f"{int(off[-1])} postings", "parallelism": "host threads"},
-            "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": n_threads, "kind": kind, "sample": sample},
-            "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    sample = (f"{desc}; each step {m} consecutive queries of the step's {n_q} (one per host thread), "
+              f"{args.steps} steps")
+    return dict(base, value=round(v, 4), ms_per_step=round(sec * 1e3, 1),
+                cpu_baseline={"value": round(v, 4), "unit": UNIT, "cores": n_threads, "kind": kind, "sample": sample},
+                e2e={"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
 
 
 # ---------------------------------------------------------------------------
@@ -664,9 +902,10 @@ def main():
     else:
         rank, world, local = dist_init(args)
         res, data = run_ours(args, rank, world, local)
+        if rank == 0 and not args.no_ref_gpu:
+            res["reference_gpu"] = reference_gpu(data)
         if rank == 0 and not args.no_cpu:
-            off, ads, qoff, qterms, _ = data
-            res["cpu_baseline"] = cpu_baseline(off, ads, qoff, qterms, args.cpu_seconds)
+            res["cpu_baseline"], res["parity"] = cpu_baseline(data, args.cpu_seconds)
         if _PG is not None:
             _PG.destroy_process_group()
         if rank != 0:
