@@ -228,6 +228,7 @@ void default_tuning(abf_index* ix) {
     // (src/AdaBool/inverted_list.h:425-458): a list of that density is
     // merged per tile by the fixed rule
     t.fixed_hybrid_min_len = uint32_t((33ull * ix->n_ads + 255) / 256);
+    t.compact_ctas_per_sm = 6;
 }
 
 void free_device(abf_index* ix) {
@@ -416,7 +417,7 @@ struct RunOpts {
 };
 
 abf_status run_compact(abf_index* ix, const abf::CompactArgs& ca, cudaStream_t s) {
-    TIMED(K_COMPACT, abf::launch_compact(ca, ix->sm_count, s));
+    TIMED(K_COMPACT, abf::launch_compact(ca, ix->sm_count, ix->tuning.compact_ctas_per_sm, s));
     return ABF_OK;
 }
 
@@ -962,6 +963,8 @@ abf_status abf_set_tuning(abf_index* ix, const abf_tuning* t) {
     if (t->scatter_blocks_per_warp == 0 || t->ctas_per_sm == 0 || t->ctas_per_sm > 32)
         return fail(ABF_ERR_INVALID, "scatter_blocks_per_warp and ctas_per_sm (<= 32) must be positive");
     if (t->probe_cap > 65536) return fail(ABF_ERR_INVALID, "probe_cap above 65536");
+    if (t->compact_ctas_per_sm == 0 || t->compact_ctas_per_sm > 6)
+        return fail(ABF_ERR_INVALID, "compact_ctas_per_sm must be 1..6");
     ix->tuning = *t;
     return ABF_OK;
 }

@@ -1500,14 +1500,14 @@ cudaError_t launch_probe(const IndexView& v, const ProbeArgs& a, const abf_tunin
     return cudaGetLastError();
 }
 
-cudaError_t launch_compact(const CompactArgs& a, int sm_count, cudaStream_t s) {
+cudaError_t launch_compact(const CompactArgs& a, int sm_count, uint32_t ctas_per_sm, cudaStream_t s) {
     const uint64_t items = uint64_t(a.n_q) * a.n_chunks;
     if (items == 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(a.status, 0, items * sizeof(uint64_t), s);
     if (e == cudaSuccess) e = cudaMemsetAsync(a.ticket, 0, sizeof(unsigned long long), s);
     if (e == cudaSuccess && a.id_counts) e = cudaMemsetAsync(a.id_counts, 0, uint64_t(a.n_q) * sizeof(uint64_t), s);
     if (e != cudaSuccess) return e;
-    compact_kernel<<<grid_for(items, sm_count, 6), 256, 0, s>>>(a);
+    compact_kernel<<<grid_for(items, sm_count, ctas_per_sm ? ctas_per_sm : 6u), 256, 0, s>>>(a);
     count_launch();
     return cudaGetLastError();
 }

@@ -232,7 +232,7 @@ cudaError_t launch_adam(float* p, const float* g, float* m, float* v, uint32_t s
                         float eps, cudaStream_t s);
 
 // clears status / ticket / id_counts on the stream, then one compaction launch
-cudaError_t launch_compact(const CompactArgs& a, int sm_count, cudaStream_t s);
+cudaError_t launch_compact(const CompactArgs& a, int sm_count, uint32_t ctas_per_sm, cudaStream_t s);
 
 // Self-test of the bounded waits: one CTA arms an mbarrier for 16 bytes that
 // no copy delivers, another looks back at a status word that no item

@@ -106,7 +106,7 @@ extern "C" abf_status abf_collect_ids_noalloc(const uint32_t* d_bitmap, uint64_t
         // the error word starts clear for every call; launch_compact clears
         // the status words, the ticket and *d_count on the stream
         if ((e = cudaMemsetAsync(ca.err, 0, sizeof(uint32_t), s)) != cudaSuccess ||
-            (e = abf::launch_compact(ca, slot.sm_count, s)) != cudaSuccess)
+            (e = abf::launch_compact(ca, slot.sm_count, 6u, s)) != cudaSuccess)
             return abf::fail(ABF_ERR_CUDA, std::string("abf_collect_ids_noalloc launch: ") + cudaGetErrorString(e));
         return ABF_OK;
     } catch (...) {

@@ -166,6 +166,8 @@ typedef struct abf_tuning {
                                  ceil(33 * n_ads / 256): the density at which the
                                  reference stores a 256-id bucket as a bitset
                                  (src/AdaBool/inverted_list.h:425-458) */
+    uint32_t compact_ctas_per_sm; /* resident CTAs per SM of the compaction (1..6, default
+                                 6); fewer leave room for another stream's kernels */
 } abf_tuning;
 
 abf_status abf_get_tuning(const abf_index* index, abf_tuning* out);
