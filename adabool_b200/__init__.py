@@ -15,8 +15,8 @@ Every call goes through libadabool.so; device buffers are torch CUDA tensors.
 from ._native import (AbfError, PATH_AUTO, PATH_HYBRID, PATH_NAMES, PATH_PROBE, PATH_TILE, PATH_UNION,
                       lib)
 from .index import (Index, Worker, Workspace, ListUnion_dense, ListUnion_sparse, BatchListUnion_dense,
-                    BatchListUnion_sparse, CollectIdsFromBitmap, launch_count)
+                    BatchListUnion_sparse, BatchCollectIds, CollectIdsFromBitmap, launch_count)
 
 __all__ = ["AbfError", "Index", "Worker", "Workspace", "ListUnion_dense", "ListUnion_sparse",
-           "BatchListUnion_dense", "BatchListUnion_sparse", "CollectIdsFromBitmap", "launch_count", "lib",
+           "BatchListUnion_dense", "BatchListUnion_sparse", "BatchCollectIds", "CollectIdsFromBitmap", "launch_count", "lib",
            "PATH_AUTO", "PATH_PROBE", "PATH_UNION", "PATH_HYBRID", "PATH_TILE", "PATH_NAMES"]

@@ -143,6 +143,7 @@ PROTOTYPES = {
     "abf_batch_list_union_dense": [vp, vp, C.c_uint32, vp],
     "abf_batch_list_union_sparse": [vp, vp, vp, C.c_uint32, vp],
     "abf_collect_ids": [vp, vp, C.c_uint64, vp, C.c_uint64, vp, vp],
+    "abf_batch_collect_ids": [vp, vp, vp, C.c_uint64, C.c_uint32, vp, C.c_uint64, vp, vp],
     "abf_collect_ids_noalloc": [vp, C.c_uint64, vp, C.c_uint64, vp, vp],
     "abf_collect_ids_noalloc_check": [vp],
     "abf_workspace_create": [vp, C.c_uint32, C.c_uint64, C.POINTER(vp)],

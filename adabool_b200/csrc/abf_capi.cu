@@ -1140,6 +1140,37 @@ abf_status abf_collect_ids(abf_index* ix, const uint32_t* d_bitmap, uint64_t n_b
     API_END
 }
 
+abf_status abf_batch_collect_ids(abf_index* ix, abf_workspace* ws, const uint32_t* d_bitmaps, uint64_t stride_words,
+                                 uint32_t n_bitmaps, uint32_t* d_ids, uint64_t ids_capacity, uint64_t* d_id_offsets,
+                                 void* stream) {
+    API_BEGIN
+    ABF_TRY(need_device(ix));
+    if (!ws || ws->ix != ix || !d_id_offsets || (n_bitmaps && !d_bitmaps) || (ids_capacity && !d_ids))
+        return fail(ABF_ERR_INVALID, "abf_batch_collect_ids: bad arguments");
+    if (n_bitmaps == 0) return ABF_OK;
+    if (n_bitmaps > ws->max_q) return fail(ABF_ERR_CAPACITY, "abf_batch_collect_ids: more bitmaps than the workspace's queries");
+    const uint64_t n_words = n_words_of(ix->n_ads);
+    if (stride_words < n_words) return fail(ABF_ERR_INVALID, "abf_batch_collect_ids: stride_words < (n_ads+31)/32");
+    CUDA_TRY(cudaSetDevice(ix->device));
+    abf::CompactArgs ca{};
+    ca.bm = d_bitmaps;
+    ca.stride = stride_words;
+    ca.n_q = n_bitmaps;
+    ca.n_bits = ix->n_ads;
+    ca.n_chunks = abf::compact_chunks(ix->n_ads);
+    ca.status = ws->scan_status;
+    ca.ticket = ws->ticket;
+    ca.ids = d_ids;
+    ca.capacity = d_ids ? ids_capacity : 0;
+    ca.id_offsets = d_id_offsets;
+    ca.id_counts = nullptr;
+    ca.err = ws->err;
+    ca.spin_limit = ws->spin_limit;
+    ABF_TRY(run_compact(ix, ca, static_cast<cudaStream_t>(stream)));
+    return ABF_OK;
+    API_END
+}
+
 // ---------------------------------------------------------------------------
 // native batch API
 // ---------------------------------------------------------------------------

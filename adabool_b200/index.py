@@ -304,6 +304,14 @@ def BatchListUnion_sparse(worker: Worker, d_res, d_qidx, res_len_per_batch_bytes
                                                    res_len_per_batch_bytes, stream_ptr(stream)))
 
 
+def BatchCollectIds(index: Index, ws: Workspace, d_bitmaps, stride_words: int, n_bitmaps: int, d_ids, d_id_offsets,
+                    stream=None) -> int:
+    """Packed ascending ids of a batch of device bitmaps (abf_batch_collect_ids)."""
+    return check(lib().abf_batch_collect_ids(index.handle, ws.handle, ptr(d_bitmaps), stride_words, n_bitmaps,
+                                             ptr(d_ids), 0 if d_ids is None else d_ids.numel(), ptr(d_id_offsets),
+                                             stream_ptr(stream)))
+
+
 def CollectIdsFromBitmap(index: Index, d_bitmap, n_bits: int, d_ids, d_count, stream=None) -> int:
     """Ascending ids of the set bits below n_bits, on the device (test/adsfilter_batch.cu:82-97)."""
     return check(lib().abf_collect_ids(index.handle, ptr(d_bitmap), n_bits, ptr(d_ids), d_ids.numel(),

@@ -241,6 +241,19 @@ abf_status abf_collect_ids(abf_index* index, const uint32_t* d_bitmap, uint64_t 
                            uint32_t* d_ids, uint64_t ids_capacity, uint64_t* d_count,
                            void* stream);
 
+/* Ascending ids of a batch of n_bitmaps device bitmaps (bitmap q at
+ * d_bitmaps + q * stride_words, (n_ads + 31) / 32 words each, bits past n_ads
+ * ignored), packed into d_ids: bitmap q's ids at d_id_offsets[q] ..
+ * d_id_offsets[q+1] (n_bitmaps + 1 offsets, written); ids past ids_capacity
+ * are not written, the offsets stay exact. One pass per bitmap (count, offset
+ * by look-back, write), with the workspace's compaction scratch (not
+ * concurrently with a batch on the same workspace); n_bitmaps at most the
+ * workspace's max_queries. Replaces the host loop of CollectIdsFromBitmap over
+ * a batch's results (test/adsfilter_batch.cu:82-97,512-519). */
+abf_status abf_batch_collect_ids(abf_index* index, abf_workspace* ws, const uint32_t* d_bitmaps,
+                                 uint64_t stride_words, uint32_t n_bitmaps, uint32_t* d_ids,
+                                 uint64_t ids_capacity, uint64_t* d_id_offsets, void* stream);
+
 /* Allocation-free variant of abf_collect_ids, with no counterpart in the
  * reference. For callers that may not allocate device memory when they
  * need the ids: an engine that owns all device memory and forbids plugins

@@ -483,3 +483,38 @@ def test_reference_kernels_agree(small):
     finally:
         H.refq_gpu_free(h)
         mixed.free()
+
+
+def test_batch_collect_ids(small):
+    """abf_batch_collect_ids over a batch of bitmaps (empty, full, random
+    densities, a stride wider than the bitmap), packed ids against the
+    definition; with a short capacity the offsets stay exact and the ids
+    that fit are written."""
+    torch = _torch()
+    ix, n_words = small["ix"], small["n_words"]
+    n_ads = small["spec"].n_ads
+    rng = np.random.default_rng(21)
+    stride = ((n_words + 3) // 4) * 4 + 8
+    dens = [0.0, 1.0, 0.5, 0.02, 0.9, 0.0001, 0.3]
+    host = np.zeros((len(dens), stride), np.uint32)
+    for i, d in enumerate(dens):
+        bits = rng.random(stride * 32) < d
+        host[i] = np.packbits(bits, bitorder="little").view(np.uint32)
+    exp = [O.collect_ids(host[i, :n_words].copy(), n_ads) for i in range(len(dens))]
+    total = sum(e.size for e in exp)
+    d_bm = torch.from_numpy(host.view(np.int32)).cuda()
+    ws = ix.workspace(len(dens), 1)
+    for cap in (total + 5, total // 2):
+        ids = torch.full((cap + 32,), -7, dtype=torch.int32, device="cuda")
+        idoff = torch.zeros(len(dens) + 1, dtype=torch.int64, device="cuda")
+        ab.BatchCollectIds(ix, ws, d_bm, stride, len(dens), ids[:cap], idoff)
+        ws.check()
+        o = idoff.cpu().numpy()
+        got = ids.cpu().numpy().view(np.uint32)
+        assert o[0] == 0 and o[-1] == total
+        flat = np.concatenate(exp)
+        for i, e in enumerate(exp):
+            assert o[i + 1] - o[i] == e.size, i
+        k = min(cap, total)
+        assert np.array_equal(got[:k], flat[:k])
+        assert (ids[cap:] == -7).all()
