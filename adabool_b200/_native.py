@@ -57,7 +57,8 @@ class Tuning(C.Structure):
                 ("probe_chunk_blocks", C.c_uint32), ("scatter_blocks_per_warp", C.c_uint32),
                 ("ctas_per_sm", C.c_uint32), ("probe_cap", C.c_uint32), ("probe_min_fraction", C.c_float),
                 ("group_min_queries", C.c_uint32), ("fixed_tile_shape", C.c_uint32),
-                ("fixed_hybrid_min_len", C.c_uint32), ("compact_ctas_per_sm", C.c_uint32)]
+                ("fixed_hybrid_min_len", C.c_uint32), ("compact_ctas_per_sm", C.c_uint32),
+                ("group_tile_words", C.c_uint32)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -229,6 +229,7 @@ void default_tuning(abf_index* ix) {
     // merged per tile by the fixed rule
     t.fixed_hybrid_min_len = uint32_t((33ull * ix->n_ads + 255) / 256);
     t.compact_ctas_per_sm = 6;
+    t.group_tile_words = 0;
 }
 
 void free_device(abf_index* ix) {
@@ -520,6 +521,15 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
     } else if (out8 && abf::dense_group_list_cap(n_dense + 1, wq, 64, 1) >= 64u * wq) {
         gw = 64;
         stages = 1;
+    } else if (out8 && t.group_tile_words == 64 && abf::dense_group_list_cap(n_dense + 1, wq, 64, 1) > 0) {
+        // 64-word tiles asked for where the window's lists do not fit beside
+        // them: one stage, the lists read from global memory
+        gw = 64;
+        stages = 1;
+    }
+    if (t.group_tile_words == 32) {
+        gw = 32;
+        stages = abf::dense_group_list_cap(n_dense + 1, wq, 32, 2) > 0 ? 2u : 1u;
     }
     if (group && (ix->dense_tmap_base != ix->dev.dense || ix->dense_tmap_rows != n_dense ||
                   ix->dense_tmap_gw != gw)) {
@@ -965,6 +975,8 @@ abf_status abf_set_tuning(abf_index* ix, const abf_tuning* t) {
     if (t->probe_cap > 65536) return fail(ABF_ERR_INVALID, "probe_cap above 65536");
     if (t->compact_ctas_per_sm == 0 || t->compact_ctas_per_sm > 6)
         return fail(ABF_ERR_INVALID, "compact_ctas_per_sm must be 1..6");
+    if (t->group_tile_words != 0 && t->group_tile_words != 32 && t->group_tile_words != 64)
+        return fail(ABF_ERR_INVALID, "group_tile_words must be 0, 32 or 64");
     ix->tuning = *t;
     return ABF_OK;
 }

@@ -168,6 +168,10 @@ typedef struct abf_tuning {
                                  (src/AdaBool/inverted_list.h:425-458) */
     uint32_t compact_ctas_per_sm; /* resident CTAs per SM of the compaction (1..6, default
                                  6); fewer leave room for another stream's kernels */
+    uint32_t group_tile_words;  /* dense group kernel tile: 0 = 64 words where a stage and
+                                 the window's lists fit shared memory, else 32; 64 = 64
+                                 words wherever one stage fits (lists then read from
+                                 global memory); 32 = always 32 */
 } abf_tuning;
 
 abf_status abf_get_tuning(const abf_index* index, abf_tuning* out);
