@@ -22,7 +22,8 @@ constexpr int O = ABF_PLANNER_OUTPUTS;
 constexpr int kMu = 0, kSd = 16, kW1 = 32, kB1 = kW1 + H * F, kW2 = kB1 + H, kB2 = kW2 + H * H, kW3 = kB2 + H,
               kB3 = kW3 + O * H, kNParams = kB3 + O;
 static_assert(kNParams == ABF_PLANNER_PARAMS, "parameter layout");
-constexpr int kFeatThreads = 128;
+constexpr int kFeatThreads = 256;
+constexpr int kFeatUnroll = 4;  // terms per thread per pass, their loads in flight together
 
 __device__ __forceinline__ uint32_t lane() { return threadIdx.x & 31u; }
 
@@ -46,7 +47,9 @@ struct FeatCtx {
 
 // The 16 features of query q, computed by the whole CTA (kFeatThreads
 // threads) into f[] in shared memory. Term ids >= n_terms are skipped;
-// repeated terms count once per occurrence.
+// repeated terms count once per occurrence. Each thread takes kFeatUnroll
+// terms per pass and issues all their table loads before using any, so a
+// query of thousands of terms costs a few memory latencies, not one per term.
 __device__ void query_features(const IndexView& ix, const uint32_t* terms, const uint64_t* q_off, uint32_t q,
                                const FeatCtx& c, float* f) {
     __shared__ double s_d[6][kFeatThreads / 32];
@@ -55,23 +58,39 @@ __device__ void query_features(const IndexView& ix, const uint32_t* terms, const
     uint32_t n = 0, mx = 0, nd = 0, nl = 0;
     double S = 0, Q = 0, Cb = 0, Lg = 0, Sd = 0, Bnd = 0;
     const double inv_ads = 1.0 / double(ix.n_ads);
-    for (uint64_t i = qb + threadIdx.x; i < qe; i += kFeatThreads) {
-        const uint32_t t = terms[i];
-        if (t >= ix.n_terms) continue;
-        const uint32_t len = __ldg(ix.term_len + t);
-        const bool dense = __ldg(ix.term_dense + t) != kNone;
-        ++n;
-        mx = max(mx, len);
-        S += len;
-        Q += double(len) * len;
-        Cb += __ldg(ix.term_cbytes + t);
-        Lg += log1p(-fmin(double(len) * inv_ads, 0.999999));
-        if (dense) {
-            ++nd;
-            Sd += len;
-        } else {
-            Bnd += __ldg(ix.term_blk + t + 1) - __ldg(ix.term_blk + t);
-            if (len < c.hybrid_min) ++nl;
+    for (uint64_t i0 = qb + threadIdx.x; i0 < qe; i0 += uint64_t(kFeatThreads) * kFeatUnroll) {
+        uint32_t t[kFeatUnroll], len[kFeatUnroll], dn[kFeatUnroll], cb[kFeatUnroll], b0[kFeatUnroll],
+            b1[kFeatUnroll];
+#pragma unroll
+        for (int u = 0; u < kFeatUnroll; ++u) {
+            const uint64_t i = i0 + uint64_t(u) * kFeatThreads;
+            t[u] = i < qe ? terms[i] : kNone;
+        }
+#pragma unroll
+        for (int u = 0; u < kFeatUnroll; ++u) {
+            const bool ok = t[u] < ix.n_terms;
+            len[u] = ok ? __ldg(ix.term_len + t[u]) : 0u;
+            dn[u] = ok ? __ldg(ix.term_dense + t[u]) : kNone;
+            cb[u] = ok ? __ldg(ix.term_cbytes + t[u]) : 0u;
+            b0[u] = ok ? __ldg(ix.term_blk + t[u]) : 0u;
+            b1[u] = ok ? __ldg(ix.term_blk + t[u] + 1) : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < kFeatUnroll; ++u) {
+            if (t[u] >= ix.n_terms) continue;
+            ++n;
+            mx = max(mx, len[u]);
+            S += len[u];
+            Q += double(len[u]) * len[u];
+            Cb += cb[u];
+            Lg += log1p(-fmin(double(len[u]) * inv_ads, 0.999999));
+            if (dn[u] != kNone) {
+                ++nd;
+                Sd += len[u];
+            } else {
+                Bnd += b1[u] - b0[u];
+                if (len[u] < c.hybrid_min) ++nl;
+            }
         }
     }
     const uint32_t w = threadIdx.x >> 5;
