@@ -70,10 +70,6 @@ def parse():
     p.add_argument("--config", default="c1")
     p.add_argument("--scale", type=float, default=1.0, help="shrink the workload (profiling / quick runs)")
     p.add_argument("--queries", type=int, default=0, help="override the query count")
-    p.add_argument("--pipeline", choices=["sub", "window"], default="sub",
-                   help="sub: every sub-batch runs the whole path (merge, scatter, compaction); window: one call "
-                        "merges the step's whole query window (the dense group kernel reads each dense bitmap once "
-                        "per step), then the sub-batches' compactions run on the streams")
     p.add_argument("--streams", type=int, default=2,
                    help="streams the sub-batches alternate over (each with its own workspace and buffers)")
     p.add_argument("--sub-batch", type=int, default=0,
@@ -278,51 +274,25 @@ def run_ours(args, rank, world, dev):
              torch.from_numpy(o.view(np.int64)).to(dev), b - a) for a, b, o, t in sbs]
     n_streams = max(1, min(args.streams, len(sbs)))
     nbuf = max(n_streams, 1 if args.no_e2e else 2)
-    window = args.pipeline == "window"
     ws = [ix.workspace(sbq, max_terms) for _ in range(nbuf)]
-    bms = [torch.empty((sbq, stride), dtype=torch.int32, device=dev) for _ in range(nbuf)] if not window else []
+    bms = [torch.empty((sbq, stride), dtype=torch.int32, device=dev) for _ in range(nbuf)]
     ids = [torch.empty(cap, dtype=torch.int32, device=dev) for _ in range(nbuf)]
     idoff = [torch.zeros(sbq + 1, dtype=torch.int64, device=dev) for _ in range(nbuf)]
     stream = torch.cuda.Stream(device=dev)
     streams = [stream] + [torch.cuda.Stream(device=dev) for _ in range(n_streams - 1)]
     fork = torch.cuda.Event()
     joins = [torch.cuda.Event() for _ in streams]
-    if window:
-        # the whole step's queries in one call: every bitmap of the window
-        d_all = (torch.from_numpy(qterms.view(np.int32)).to(dev),
-                 torch.from_numpy(np.ascontiguousarray(qoff, np.uint64).view(np.int64)).to(dev))
-        ws_all = ix.workspace(n_q, int(qoff[-1]) + 1)
-        bm_all = torch.empty((n_q, stride), dtype=torch.int32, device=dev)
-        bms = [bm_all]
-
-    def union_all(s):
-        """window pipeline: bitmaps of every query of the step (no ids)."""
-        if window:
-            ix.batch_run(ws_all, d_all[0], d_all[1], n_q, bm_all, stride, path=path, stream=s)
-
-    def sub(i, k, s, with_ids=True):
-        """sub-batch i on buffer set k: the whole path (sub pipeline), or the
-        compaction of its rows of the window's bitmaps (window pipeline)."""
-        a, b = sbs[i][0], sbs[i][1]
-        dt, do, nq = d_in[i]
-        if window:
-            if with_ids:
-                ab.BatchCollectIds(ix, ws[k], bm_all[a:b], stride, nq, ids[k], idoff[k], stream=s)
-        elif with_ids:
-            ix.batch_run(ws[k], dt, do, nq, bms[k], stride, path=path, d_ids=ids[k], d_id_offsets=idoff[k], stream=s)
-        else:
-            ix.batch_run(ws[k], dt, do, nq, bms[k], stride, path=path, stream=s)
 
     def step():
         # sub-batch i runs on stream i % n with buffer set i % n, so one
         # sub-batch's compaction overlaps the next one's merge and scatter
-        union_all(stream)
         fork.record(stream)
         for s in streams[1:]:
             s.wait_event(fork)
-        for i in range(len(d_in)):
+        for i, (dt, do, nq) in enumerate(d_in):
             k = i % n_streams
-            sub(i, k, streams[k])
+            ix.batch_run(ws[k], dt, do, nq, bms[k], stride, path=path, d_ids=ids[k], d_id_offsets=idoff[k],
+                         stream=streams[k])
         for s, e in zip(streams[1:], joins[1:]):
             e.record(s)
             stream.wait_event(e)
@@ -333,17 +303,15 @@ def run_ours(args, rank, world, dev):
     sums = np.zeros((n_par, 2), np.uint64)
     with torch.cuda.stream(stream):
         counts = np.zeros(n_q, np.uint64)
-        union_all(stream)
-        for i, ((a, b, _, _), (dt, do, nq)) in enumerate(zip(sbs, d_in)):
-            sub(i, 0, stream)
+        for (a, b, _, _), (dt, do, nq) in zip(sbs, d_in):
+            ix.batch_run(ws[0], dt, do, nq, bms[0], stride, path=path, d_ids=ids[0], d_id_offsets=idoff[0],
+                         stream=stream)
             stream.synchronize()
             o = idoff[0][:nq + 1].cpu().numpy()
             counts[a:b] = np.diff(o)
             for i in range(a, min(b, n_par)):
                 sums[i] = id_checksums(ids[0][int(o[i - a]):], int(o[i - a + 1] - o[i - a]), torch)
     ws[0].check(stream)
-    if window:
-        ws_all.check(stream)
 
     for _ in range(args.warmup):
         step()
@@ -363,7 +331,7 @@ def run_ours(args, rank, world, dev):
     ms_total = e0.elapsed_time(e1)
     ms_step = dist_max(ms_total / args.steps, world)
     dist_barrier(world)
-    for w in ws + ([ws_all] if window else []):
+    for w in ws:
         w.check(stream)
 
     # per-kernel CUDA-event times for the roofline: the same K steps once
@@ -372,9 +340,9 @@ def run_ours(args, rank, world, dev):
     ix.profile(True)
     ix.profile_read()
     for _ in range(args.steps):
-        union_all(stream)
-        for i in range(len(d_in)):
-            sub(i, 0, stream)
+        for (dt, do, nq) in d_in:
+            ix.batch_run(ws[0], dt, do, nq, bms[0], stride, path=path, d_ids=ids[0], d_id_offsets=idoff[0],
+                         stream=stream)
     stream.synchronize()
     kern = ix.profile_read()
     ix.profile(False)
@@ -384,9 +352,8 @@ def run_ours(args, rank, world, dev):
     reps = max(1, args.steps // 2)
     with torch.cuda.stream(stream):
         def bm_step():
-            union_all(stream)
-            for i in range(len(d_in)):
-                sub(i, 0, stream, with_ids=False)
+            for (dt, do, nq) in d_in:
+                ix.batch_run(ws[0], dt, do, nq, bms[0], stride, path=path, stream=stream)
         bm_step()
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         f0.record(stream)
@@ -399,8 +366,7 @@ def run_ours(args, rank, world, dev):
     # ---- e2e through the public API from pinned host buffers ----
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(args, ix, sbs, ws, bms, ids, idoff, stride, path, dev, world, n_q,
-                      (d_all, ws_all, bm_all, qoff, qterms) if window else None)
+        e2e = run_e2e(args, ix, sbs, ws, bms, ids, idoff, stride, path, dev, world, n_q)
 
     # ---- physical bytes per kernel (roofline numerators) ----
     # every kernel is charged the bytes its design must move once: the dense
@@ -496,7 +462,7 @@ def run_ours(args, rank, world, dev):
         "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded Zipf lists, lognormal queries)",
         "config": workload_config(cfg, int(st["n_postings"]), n_q),
-        "execution": {"path": args.path, "parallelism": f"replicas{world}", "pipeline": args.pipeline,
+        "execution": {"path": args.path, "parallelism": f"replicas{world}",
                       "sub_batch": args.sub_batch, "streams": n_streams, "index_bytes": st["device_bytes"],
                       "tuning": dict(ix.tuning.as_dict(), dense_div=ix.dense_div), "autotune": tune_info},
         "postings_per_s": round(postings * world / (ms_step / 1e3), 1),
@@ -516,9 +482,8 @@ def run_ours(args, rank, world, dev):
                      dev=dev)
 
 
-def run_e2e(args, ix, sbs, ws, bms, ids, idoff, stride, path, dev, world, n_q, window=None):
+def run_e2e(args, ix, sbs, ws, bms, ids, idoff, stride, path, dev, world, n_q):
     import torch
-    import adabool_b200 as ab
     streams = [torch.cuda.Stream(device=dev) for _ in range(2)]
     maxt = max(int(t.size) for _, _, _, t in sbs) + 1
     maxq = max(b - a for a, b, _, _ in sbs) + 1
@@ -534,40 +499,22 @@ def run_e2e(args, ix, sbs, ws, bms, ids, idoff, stride, path, dev, world, n_q, w
         e.record(streams[0])
     h2d = d2h = 0
 
-    if window:
-        d_all, ws_all, bm_all, qoff_all, qterms_all = window
-        h_all = [torch.from_numpy(np.ascontiguousarray(qterms_all, np.uint32).view(np.int32)).pin_memory(),
-                 torch.from_numpy(np.ascontiguousarray(qoff_all, np.uint64).view(np.int64)).pin_memory()]
-        union_done = torch.cuda.Event()
-
     def one_step():
         nonlocal h2d, d2h
         h2d = d2h = 0
-        if window:  # every query's terms in one copy, the window's bitmaps in one call
-            with torch.cuda.stream(streams[0]):
-                d_all[0][:h_all[0].numel()].copy_(h_all[0], non_blocking=True)
-                d_all[1].copy_(h_all[1], non_blocking=True)
-                ix.batch_run(ws_all, d_all[0], d_all[1], n_q, bm_all, stride, path=path, stream=streams[0])
-                union_done.record(streams[0])
-            streams[1].wait_event(union_done)
-            h2d += h_all[0].numel() * 4 + h_all[1].numel() * 8
         for i, (a, b, o, t) in enumerate(sbs):
             k = i % 2
             s = streams[k]
             nq = b - a
             done[k].synchronize()  # pinned buffers of set k are free again
             with torch.cuda.stream(s):
-                if window:
-                    ab.BatchCollectIds(ix, ws[k], bm_all[a:b], stride, nq, ids[k], idoff[k], stream=s)
-                else:
-                    d_terms[k][:h_terms[i].numel()].copy_(h_terms[i], non_blocking=True)
-                    d_offs[k][:nq + 1].copy_(h_offs[i], non_blocking=True)
-                    ix.batch_run(ws[k], d_terms[k], d_offs[k], nq, bms[k], stride, path=path, d_ids=ids[k],
-                                 d_id_offsets=idoff[k], stream=s)
+                d_terms[k][:h_terms[i].numel()].copy_(h_terms[i], non_blocking=True)
+                d_offs[k][:nq + 1].copy_(h_offs[i], non_blocking=True)
+                ix.batch_run(ws[k], d_terms[k], d_offs[k], nq, bms[k], stride, path=path, d_ids=ids[k],
+                             d_id_offsets=idoff[k], stream=s)
                 h_idoff[k][:nq + 1].copy_(idoff[k][:nq + 1], non_blocking=True)
                 ev_off[k].record(s)
-            if not window:
-                h2d += t.size * 4 + (nq + 1) * 8
+            h2d += t.size * 4 + (nq + 1) * 8
             ev_off[k].synchronize()
             tot = int(h_idoff[k][nq])
             with torch.cuda.stream(s):
