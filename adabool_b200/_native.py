@@ -151,6 +151,7 @@ PROTOTYPES = {
     "abf_workspace_free": [vp],
     "abf_workspace_check": [vp, vp],
     "abf_workspace_set_wait_limit": [vp, C.c_uint32],
+    "abf_workspace_paths": [vp, u8p, C.c_uint32, vp],
     "abf_workspace_selftest_waits": [vp, C.c_uint32, vp],
     "abf_batch_run": [vp, vp, C.POINTER(Batch), vp],
     "abf_query": [vp, u32p, C.c_uint32, C.c_int, vp, vp, C.c_uint64, vp, vp],

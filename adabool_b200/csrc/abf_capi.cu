@@ -460,12 +460,10 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
     pa.q_dmode = ws->q_dmode;
     pa.tile_list = ws->tile_list;
     pa.n_tile_list = ws->n_tile_list;
-    if (!b->d_paths && b->path == ABF_PATH_AUTO && ix->dev.planner) {
-        // learned planner: per-query path from the fused feature + MLP kernel
-        TIMED(K_PLANNER, abf::launch_planner(v, ix->dev.planner, b->d_terms, b->d_offsets, b->n_queries,
-                                             t.heavy_min_len, ix->n_postings, nullptr, nullptr, ws->auto_paths, s));
-        pa.paths = ws->auto_paths;
-    }
+    // learned planner: the plan kernel runs its feature + MLP code for the
+    // ABF_PATH_AUTO queries (no separate launch)
+    pa.planner = ix->dev.planner;
+    pa.n_postings = ix->n_postings;
     TIMED(K_PLAN, abf::launch_plan(v, pa, s));
     abf::QueueArgs qa{ws->lcnt, ws->lpref_q, b->n_queries};
     TIMED(K_QUEUE, abf::launch_queue_scan(qa, s));
@@ -1237,6 +1235,19 @@ abf_status abf_workspace_check(abf_workspace* w, void* stream) {
     CUDA_TRY(cudaStreamSynchronize(s));
     if (err & abf::kErrTermRange) return fail(ABF_ERR_CAPACITY, "a query's term offsets exceed the workspace's max_terms");
     if (err) return fail(ABF_ERR_TIMEOUT, "a bounded device wait gave up (code " + std::to_string(err) + ")");
+    return ABF_OK;
+    API_END
+}
+
+abf_status abf_workspace_paths(abf_workspace* w, uint8_t* h_paths, uint32_t n, void* stream) {
+    API_BEGIN
+    if (!w || (n && !h_paths)) return fail(ABF_ERR_INVALID, "abf_workspace_paths: bad arguments");
+    if (n > w->max_q) return fail(ABF_ERR_CAPACITY, "abf_workspace_paths: more queries than the workspace holds");
+    if (n == 0) return ABF_OK;
+    CUDA_TRY(cudaSetDevice(w->ix->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    CUDA_TRY(cudaMemcpyAsync(h_paths, w->path_out, n, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
     return ABF_OK;
     API_END
 }

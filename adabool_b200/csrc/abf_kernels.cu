@@ -13,6 +13,7 @@
 //   count/scan/write  <- the host loop CollectIdsFromBitmap
 //       (test/adsfilter_batch.cu:82-97)
 #include "abf_kernels.cuh"
+#include "abf_planner_dev.cuh"
 
 #include <cuda.h>
 #include <cstring>
@@ -250,6 +251,8 @@ __global__ void __launch_bounds__(256) plan_kernel(IndexView ix, PlanArgs a) {
     __shared__ unsigned long long s_red[8];
     __shared__ uint32_t s_path, s_max;
     __shared__ uint32_t s_mask[2048];  // the query's dense bitmaps (n_dense <= 65535)
+    __shared__ plan_dev::PlannerSmem s_pl;
+    static_assert(plan_dev::kFeatThreads == 256, "the planner code runs with the plan kernel's 256 threads");
     const uint32_t tid = threadIdx.x;
     for (uint32_t q = blockIdx.x; q < a.n_q; q += gridDim.x) {
         uint64_t qb = a.q_off[q], qe = a.q_off[q + 1];
@@ -259,7 +262,11 @@ __global__ void __launch_bounds__(256) plan_kernel(IndexView ix, PlanArgs a) {
             qe = qb = 0;
         }
         uint32_t path = a.paths ? a.paths[q] : a.path_uniform;
-        if (path == ABF_PATH_AUTO) {
+        if (path == ABF_PATH_AUTO && a.planner) {
+            // learned planner: features + MLP of this query, inline
+            path = plan_dev::planner_path(ix, a.planner, a.terms, a.q_off, q,
+                                          plan_dev::FeatCtx{a.hybrid_min, a.n_postings, a.n_q}, s_pl);
+        } else if (path == ABF_PATH_AUTO) {
             // fixed rule: probe when the query's lists cover more than
             // probe_min_frac of all blocks; else HYBRID when one of its lists
             // has at least fixed_hybrid_min postings; else list-union

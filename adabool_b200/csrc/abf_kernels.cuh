@@ -51,6 +51,9 @@ struct PlanArgs {
     const uint8_t* paths;     // per-query abf_path or null
     uint32_t path_uniform;    // abf_path when paths is null
     uint32_t hybrid_min;      // HYBRID merge threshold (postings)
+    const float* planner;     // installed planner parameters (ABF_PLANNER_PARAMS) or null: with
+                              // them, ABF_PATH_AUTO queries take the MLP's choice
+    uint64_t n_postings;      // index postings (a planner feature)
     float probe_min_frac;     // fixed rule: probe when touched blocks / all blocks > this
     uint32_t fixed_hybrid_min;  // fixed rule otherwise: HYBRID when a list has >= this many
                                 // postings (0: never), else UNION

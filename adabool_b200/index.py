@@ -76,6 +76,12 @@ class Workspace:
     def check(self, stream=None):
         check(lib().abf_workspace_check(self._h, stream_ptr(stream)))
 
+    def paths(self, n: int, stream=None) -> np.ndarray:
+        """abf_path each of the last batch's first n queries ran on."""
+        out = np.zeros(n, np.uint8)
+        check(lib().abf_workspace_paths(self._h, ptr(out, N.u8p), n, stream_ptr(stream)))
+        return out
+
     def set_wait_limit(self, polls: int):
         """Polls of every bounded device wait of this workspace's kernels."""
         check(lib().abf_workspace_set_wait_limit(self._h, int(polls)))

@@ -298,6 +298,12 @@ abf_status abf_workspace_free(abf_workspace* ws);
  * query's term offsets exceeded the workspace. */
 abf_status abf_workspace_check(abf_workspace* ws, void* stream);
 
+/* The abf_path each of the first n queries of the workspace's last batch ran
+ * on (after the planner or the fixed rule resolved ABF_PATH_AUTO, and after
+ * probe queries beyond probe_cap fell back to UNION), into a host array;
+ * synchronises the stream. No reference counterpart. */
+abf_status abf_workspace_paths(abf_workspace* ws, uint8_t* h_paths, uint32_t n, void* stream);
+
 /* Bounded device waits. The kernels launched with this workspace poll a
  * compaction look-back word or an mbarrier at most `polls` times (default
  * 2^22, well over a second) before they give up, set the workspace's error

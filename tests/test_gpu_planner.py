@@ -123,14 +123,21 @@ def test_planner_choices_and_bit_exact_auto_batches(env):
         stride = (n_words + 3) // 4 * 4
         ws = ix.workspace(n, int(qoff[-1]))
         bms = torch.empty((n, stride), dtype=torch.int32, device="cuda")
+        ix.set_tuning(probe_cap=64)  # every probe choice gets a probe slot (no fallback to UNION)
         ix.batch_run(ws, dt, do, n, bms, stride, path=ab.PATH_AUTO)
         ws.check()
+        # the plan kernel's inline planner picks what the planner kernel picks
+        N.check(ab.lib().abf_planner_predict(ix.handle, N.ptr(dt), N.ptr(do), n, None, N.ptr(paths), None))
+        torch.cuda.synchronize()
+        assert np.array_equal(ws.paths(n), paths.cpu().numpy())
+        assert len(np.unique(ws.paths(n))) >= 2  # the random weights favour more than one path
         got = bms.cpu().numpy().view(np.uint32)
         for i in range(n):
             e = O.ids_to_bitmap(O.kway_union(env["off"], env["ads"], qt[qoff[i]:qoff[i + 1]]), n_words)
             assert np.array_equal(got[i, :n_words], e), i
     finally:
         P.uninstall(ix)
+        ix.set_tuning(probe_cap=32)
 
 
 def test_collect_labels_shapes(env):
