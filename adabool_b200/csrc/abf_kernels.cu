@@ -246,7 +246,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 // ---------------------------------------------------------------------------
 // planning
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) plan_kernel(IndexView ix, PlanArgs a) {
+__global__ void __launch_bounds__(256, 4) plan_kernel(IndexView ix, PlanArgs a) {
     __shared__ uint32_t s_warp[32];
     __shared__ unsigned long long s_red[8];
     __shared__ uint32_t s_path, s_max;
@@ -1144,28 +1144,20 @@ constexpr uint32_t kIdBuf = 1024 + 8;  // one unit's ids plus the 16-byte alignm
 
 // Ids of one unit into dst[0 .. tot): lane l holds word l of the unit in v
 // and the ids of the lower lanes' words in ex; id0 = first id of the unit +
-// lane. Dense units walk the 32 words two at a time: lanes 0-15 take bits
-// 2j, 2j+1 of the even word, lanes 16-31 those of the odd word, so one pair
-// of shuffles serves two words (half the shuffles and loop overhead of one
-// lane per bit); sparse ones visit only the non-zero words, one lane per bit.
+// lane. Dense units walk all 32 words without bookkeeping; sparse ones
+// visit only the non-zero words. (Two words per shuffle pair, 16 lanes per
+// word, measured 7 % faster on uniformly random 75 %-dense bitmaps but no
+// faster on the c1 bitmaps, where saturated words put both half-warps'
+// stores on the same banks.)
 template <bool kDense, typename Store>
 __device__ __forceinline__ void expand_unit(uint32_t v, uint32_t ex, uint32_t id0, uint32_t lt, uint32_t mybit,
                                             Store store) {
     if (kDense) {
-        const uint32_t lane = lane_id();
-        const uint32_t half = lane >> 4, j = lane & 15u;
-        const uint32_t below = (1u << (2u * j)) - 1u;               // bits under this lane's pair
-        const uint32_t base = id0 - lane + half * 32u + 2u * j;     // id of bit 2j of word `half`
-#pragma unroll 4
-        for (uint32_t i = 0; i < 16u; ++i) {
-            const uint32_t w = 2u * i + half;
+#pragma unroll 8
+        for (uint32_t w = 0; w < 32u; ++w) {
             const uint32_t word = __shfl_sync(kFull, v, w);
             const uint32_t pos = __shfl_sync(kFull, ex, w);
-            const uint32_t b2 = (word >> (2u * j)) & 3u;
-            const uint32_t p = pos + __popc(word & below);
-            const uint32_t id = base + i * 64u;
-            if (b2 & 1u) store(p, id);
-            if (b2 & 2u) store(p + (b2 & 1u), id + 1u);
+            if (word & mybit) store(pos + __popc(word & lt), id0 + w * 32u);
         }
     } else {
         uint32_t nz = __ballot_sync(kFull, v != 0u);

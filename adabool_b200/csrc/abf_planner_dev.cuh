@@ -108,7 +108,9 @@ __device__ void query_features(const IndexView& ix, const uint32_t* terms, const
         s_d[0][w] = S; s_d[1][w] = Q; s_d[2][w] = Cb; s_d[3][w] = Lg; s_d[4][w] = Sd; s_d[5][w] = Bnd;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    // each of the first 16 threads sums the warps' partials and computes one
+    // feature (the transcendentals run side by side, not one after another)
+    if (threadIdx.x < F) {
         n = nd = nl = mx = 0;
         S = Q = Cb = Lg = Sd = Bnd = 0;
         for (int k = 0; k < kFeatThreads / 32; ++k) {
@@ -116,24 +118,30 @@ __device__ void query_features(const IndexView& ix, const uint32_t* terms, const
             S += s_d[0][k]; Q += s_d[1][k]; Cb += s_d[2][k]; Lg += s_d[3][k]; Sd += s_d[4][k]; Bnd += s_d[5][k];
         }
         const double nn = n > 0 ? double(n) : 1.0;
-        const double mean = S / nn;
-        const double var = fmax(Q / nn - mean * mean, 0.0);
-        f[0] = float(log1p(double(n)));
-        f[1] = float(log1p(S));
-        f[2] = float(log1p(double(mx)));
-        f[3] = float(log1p(mean));
-        f[4] = float(log1p(sqrt(var)));
-        f[5] = float(log1p(Cb));
-        f[6] = float(1.0 - exp(Lg));
-        f[7] = float(log1p(double(nd)));
-        f[8] = float(Sd / fmax(S, 1.0));
-        f[9] = float(log1p(Bnd));
-        f[10] = float(S / double(c.n_postings ? c.n_postings : 1));
-        f[11] = float(log1p(double(nl)));
-        f[12] = float(double(q) / double(c.n_q ? c.n_q : 1));
-        f[13] = float(log1p(double(c.n_q)));
-        f[14] = float(double(mx) * inv_ads);
-        f[15] = 1.0f;
+        double r;
+        switch (threadIdx.x) {
+            case 0: r = log1p(double(n)); break;
+            case 1: r = log1p(S); break;
+            case 2: r = log1p(double(mx)); break;
+            case 3: r = log1p(S / nn); break;
+            case 4: {
+                const double mean = S / nn;
+                r = log1p(sqrt(fmax(Q / nn - mean * mean, 0.0)));
+                break;
+            }
+            case 5: r = log1p(Cb); break;
+            case 6: r = 1.0 - exp(Lg); break;
+            case 7: r = log1p(double(nd)); break;
+            case 8: r = Sd / fmax(S, 1.0); break;
+            case 9: r = log1p(Bnd); break;
+            case 10: r = S / double(c.n_postings ? c.n_postings : 1); break;
+            case 11: r = log1p(double(nl)); break;
+            case 12: r = double(q) / double(c.n_q ? c.n_q : 1); break;
+            case 13: r = log1p(double(c.n_q)); break;
+            case 14: r = double(mx) * inv_ads; break;
+            default: r = 1.0; break;
+        }
+        f[threadIdx.x] = float(r);
     }
     __syncthreads();
 }
