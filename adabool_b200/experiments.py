@@ -158,27 +158,34 @@ def planner_experiment(n_train: int = 66_667, batch_config: str = "c2", reps: in
     import ctypes as C
     Lb = N.lib()
 
-    def one(i):
-        b = N.Batch(N.ptr(dt), C.c_void_p(do.data_ptr() + 8 * i), 1, None, int(paths_of[choice_fx[i]]), N.ptr(bm1),
+    def one(i, choice):
+        b = N.Batch(N.ptr(dt), C.c_void_p(do.data_ptr() + 8 * i), 1, None, int(paths_of[choice[i]]), N.ptr(bm1),
                     stride, None, 0, None)
         N.check(Lb.abf_batch_run(ix.handle, ws.handle, C.byref(b), N.stream_ptr(s)))
 
-    for i in range(min(m, 16)):
-        one(i)
-    s.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(s)
-    for i in range(m):
-        one(i)
-    e1.record(s)
-    e1.synchronize()
-    pq_ms = e0.elapsed_time(e1)
+    def per_query_ms(choice):
+        for i in range(min(m, 16)):
+            one(i, choice)
+        s.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for i in range(m):
+            one(i, choice)
+        e1.record(s)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    pq_ms = per_query_ms(choice_fx)
     for i in range(0, m, max(1, m // 32)):  # per-query results equal the batch rows
-        one(i)
+        one(i, choice_fx)
         s.synchronize()
         mism += int(not torch.equal(bm1[:ix.n_words], planner_bm[i, :ix.n_words]))
     per_query = {"queries": m, "ms": pq_ms, "queries_per_s": m / (pq_ms / 1e3),
                  "note": "abf_batch_run with one query per call, fixed-rule path, back to back on one stream"}
+    # the same per-query path with the threshold fitted to this library's own
+    # labels instead of the reference's crossover (a stronger fixed rule)
+    pq_lab_ms = per_query_ms(P.fixed_rule_choice(ix, qoff, qt, tau_labels, hyb_min))
+    per_query_lab = {"queries": m, "ms": pq_lab_ms, "queries_per_s": m / (pq_lab_ms / 1e3), "tau": tau_labels}
     P.uninstall(ix)
     return {
         "batch_config": batch_config, "n_queries": n, "terms": int(qoff[-1]),
@@ -187,6 +194,9 @@ def planner_experiment(n_train: int = 66_667, batch_config: str = "c2", reps: in
                   "epochs": tr.epochs},
         "fixed_rule": {"tau": tau, "hybrid_min_len": hyb_min, "tau_from": tau_info, "tau_from_labels": tau_labels},
         "regret": regret, "batch": batch, "per_query_fixed": per_query,
+        "per_query_fixed_label_tau": per_query_lab,
+        "speedup_planner_batch_over_per_query_fixed_label_tau":
+            batch["planner"]["queries_per_s"] / per_query_lab["queries_per_s"],
         "speedup_planner_over_always_hybrid_batch":
             batch["planner"]["queries_per_s"] / batch["always_hybrid"]["queries_per_s"],
         "speedup_planner_batch_over_per_query_fixed": batch["planner"]["queries_per_s"] / per_query["queries_per_s"],
