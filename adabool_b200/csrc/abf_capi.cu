@@ -56,8 +56,8 @@ using abf::fail;
 namespace {
 
 // ---- kernel timing (abf_profile_enable / abf_profile_read) ----
-enum Kid { K_PLAN, K_QUEUE, K_PROBE_BITS, K_TILE, K_SCATTER, K_PROBE, K_COMPACT, K_PLANNER, K_GROUP, K_NKERNELS };
-const char* const kKernelNames[K_NKERNELS] = {"plan",  "queue_scan", "probe_bits", "tile_union", "scatter_union",
+enum Kid { K_PLAN, K_QUEUE, K_TILE, K_SCATTER, K_PROBE, K_COMPACT, K_PLANNER, K_GROUP, K_NKERNELS };
+const char* const kKernelNames[K_NKERNELS] = {"plan",  "queue_scan", "tile_union", "scatter_union",
                                               "probe", "compact",    "planner",    "dense_group"};
 
 struct Profiler {
@@ -464,16 +464,13 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
     // ABF_PATH_AUTO queries (no separate launch)
     pa.planner = ix->dev.planner;
     pa.n_postings = ix->n_postings;
+    pa.probe_bm = ws->probe_bm;
+    pa.probe_stride = ws->probe_stride;
     TIMED(K_PLAN, abf::launch_plan(v, pa, s));
     abf::QueueArgs qa{ws->lcnt, ws->lpref_q, b->n_queries};
     TIMED(K_QUEUE, abf::launch_queue_scan(qa, s));
+    // the probe queries' term bitmaps are written by their plan CTAs
     const bool maybe_probe = ws->probe_cap > 0 && (b->d_paths || b->path == ABF_PATH_PROBE || b->path == ABF_PATH_AUTO);
-    if (maybe_probe) {
-        CUDA_TRY(cudaMemsetAsync(ws->probe_bm, 0, uint64_t(ws->probe_cap) * ws->probe_stride * 4u, s));
-        abf::ProbeBitsArgs pb{b->d_terms, b->d_offsets, ws->probe_list, ws->n_probe, ws->probe_bm, ws->probe_stride,
-                              ix->n_terms};
-        TIMED(K_PROBE_BITS, abf::launch_probe_bits(pb, ws->probe_cap, s));
-    }
     abf::TileArgs ta{};
     ta.tile_cls = ws->tile_cls;
     ta.q_off = b->d_offsets;

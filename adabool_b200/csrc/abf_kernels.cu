@@ -249,7 +249,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 __global__ void __launch_bounds__(256, 4) plan_kernel(IndexView ix, PlanArgs a) {
     __shared__ uint32_t s_warp[32];
     __shared__ unsigned long long s_red[8];
-    __shared__ uint32_t s_path, s_max;
+    __shared__ uint32_t s_path, s_max, s_slot;
     __shared__ uint32_t s_mask[2048];  // the query's dense bitmaps (n_dense <= 65535)
     __shared__ plan_dev::PlannerSmem s_pl;
     static_assert(plan_dev::kFeatThreads == 256, "the planner code runs with the plan kernel's 256 threads");
@@ -290,16 +290,31 @@ __global__ void __launch_bounds__(256, 4) plan_kernel(IndexView ix, PlanArgs a) 
                                                                       : ABF_PATH_UNION;
         }
         if (tid == 0) {
+            s_slot = kNone;
             if (path == ABF_PATH_PROBE) {
                 const uint32_t slot = atomicAdd(a.n_probe, 1u);
-                if (slot < a.probe_cap) a.probe_list[slot] = q;
-                else path = ABF_PATH_UNION;  // no probe slot left: same result by list-union
+                if (slot < a.probe_cap) {
+                    a.probe_list[slot] = q;
+                    s_slot = slot;
+                } else {
+                    path = ABF_PATH_UNION;  // no probe slot left: same result by list-union
+                }
             }
             s_path = path;
         }
         __syncthreads();
         path = s_path;
         const bool probe = path == ABF_PATH_PROBE;
+        if (probe && a.probe_bm) {
+            // the probe slot's term bitmap: zeroed, then this query's terms
+            uint32_t* bm = a.probe_bm + uint64_t(s_slot) * a.probe_stride;
+            for (uint64_t w = tid; w < a.probe_stride; w += 256) bm[w] = 0u;
+            __syncthreads();
+            for (uint64_t i = qb + tid; i < qe; i += 256) {
+                const uint32_t t = a.terms[i];
+                if (t < ix.n_terms) atomicOr(bm + (t >> 5), 1u << (t & 31u));
+            }
+        }
         // merge threshold: TILE merges every list, HYBRID the long ones,
         // UNION only those with a dense bitmap, PROBE none
         const uint32_t hm = path == ABF_PATH_TILE ? 0u
@@ -413,17 +428,6 @@ __global__ void __launch_bounds__(1024) queue_scan_kernel(QueueArgs a) {
         __syncthreads();
     }
     if (tid == 0) a.q_light_pref[a.n_q] = s_carry;
-}
-
-__global__ void __launch_bounds__(256) probe_bits_kernel(ProbeBitsArgs a) {
-    const uint32_t slot = blockIdx.x;
-    if (slot >= *a.n_probe) return;
-    const uint32_t q = a.probe_list[slot];
-    uint32_t* bm = a.qbm + slot * a.qbm_stride;
-    for (uint64_t i = a.q_off[q] + threadIdx.x; i < a.q_off[q + 1]; i += blockDim.x) {
-        const uint32_t t = a.terms[i];
-        if (t < a.n_terms) atomicOr(bm + (t >> 5), 1u << (t & 31u));
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1343,13 +1347,6 @@ cudaError_t launch_plan(const IndexView& v, const PlanArgs& a, cudaStream_t s) {
 
 cudaError_t launch_queue_scan(const QueueArgs& a, cudaStream_t s) {
     queue_scan_kernel<<<1, 1024, 0, s>>>(a);
-    count_launch();
-    return cudaGetLastError();
-}
-
-cudaError_t launch_probe_bits(const ProbeBitsArgs& a, uint32_t probe_cap, cudaStream_t s) {
-    if (probe_cap == 0) return cudaSuccess;
-    probe_bits_kernel<<<probe_cap, 256, 0, s>>>(a);
     count_launch();
     return cudaGetLastError();
 }

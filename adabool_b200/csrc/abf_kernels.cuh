@@ -1,11 +1,12 @@
 // Kernel argument blocks and launchers of libadabool (sm_100a).
 //
 // Kernels (all integer, HBM/L2 bound):
-//   plan_kernel        per query: resolve the path, split lists into merged
-//                      (long) and scattered (short), prefix the short lists'
-//                      block counts, claim bitmap-probe slots
+//   plan_kernel        per query: resolve the path (given, the learned
+//                      planner's inline, or the fixed rule), split lists into
+//                      merged (long) and scattered (short), prefix the short
+//                      lists' block counts, claim a bitmap-probe slot and
+//                      write the probe query's term bitmap
 //   queue_scan_kernel  exclusive scan of the per-query scattered block counts
-//   probe_bits_kernel  term bitmaps of the queries routed to the probe
 //   tile_union_kernel  list-union, merge variant: one CTA owns a tile of one
 //                      query's output bitmap in shared memory, decodes every
 //                      block of the long lists that overlaps the tile, ORs
@@ -63,6 +64,8 @@ struct PlanArgs {
     uint32_t* probe_list;     // out: probe slot -> query
     uint32_t* n_probe;        // in/out: zeroed before launch
     uint32_t probe_cap;
+    uint32_t* probe_bm;       // optional: probe slot s's term bitmap at probe_bm + s * probe_stride
+    uint64_t probe_stride;    // words; written (zeroed, then the query's terms) by the query's CTA
     uint8_t* path_out;        // out (optional): resolved path per query
     uint64_t max_terms;       // term slots of the scratch arrays; queries past it get no work
     uint32_t* err;            // device error flag (optional)
@@ -91,16 +94,6 @@ struct QueueArgs {
     const uint64_t* q_light_cnt;
     uint64_t* q_light_pref;   // n_q + 1
     uint32_t n_q;
-};
-
-struct ProbeBitsArgs {
-    const uint32_t* terms;
-    const uint64_t* q_off;
-    const uint32_t* probe_list;
-    const uint32_t* n_probe;
-    uint32_t* qbm;            // probe_cap x qbm_stride words, zeroed before launch
-    uint64_t qbm_stride;
-    uint32_t n_terms;
 };
 
 struct TileArgs {
@@ -217,7 +210,6 @@ uint32_t dense_group_list_cap(uint32_t n_rows, uint32_t n_q, uint32_t gw, uint32
 cudaError_t launch_dense_group(const void* tmaps, uint32_t gw, const DenseGroupArgs& a, int sm_count,
                                cudaStream_t s);
 cudaError_t launch_queue_scan(const QueueArgs& a, cudaStream_t s);
-cudaError_t launch_probe_bits(const ProbeBitsArgs& a, uint32_t probe_cap, cudaStream_t s);
 cudaError_t launch_tile_union(const IndexView& v, const TileArgs& a, const abf_tuning& t, int sm_count,
                               cudaStream_t s);
 cudaError_t launch_scatter(const IndexView& v, const ScatterArgs& a, const abf_tuning& t, int sm_count,
