@@ -143,6 +143,8 @@ struct abf_workspace {
     uint32_t* err = nullptr;
     uint32_t* tile_list = nullptr;  // queries the merge kernel visits beside the dense group kernel
     uint32_t* n_tile_list = nullptr;
+    uint32_t* sat = nullptr;        // per query: the dense group kernel's all-ones tiles, one bit each
+    uint32_t sat_stride = 0;        // words per query (tiles of 32 words over n_ads)
     uint32_t* q_terms = nullptr;  // single-query staging (abf_query)
     uint64_t* q_off = nullptr;
     uint32_t spin_limit = abf::kDefaultSpinLimit;  // polls of every bounded device wait
@@ -350,6 +352,7 @@ void ws_release(abf_workspace* w) {
     dev_free(w->err);
     dev_free(w->tile_list);
     dev_free(w->n_tile_list);
+    dev_free(w->sat);
     dev_free(w->q_terms);
     dev_free(w->q_off);
 }
@@ -362,6 +365,7 @@ abf_status ws_alloc(abf_index* ix, uint32_t max_q, uint64_t max_terms, uint64_t 
     w->probe_stride = round4(n_words_of(ix->n_terms));
     w->chunks_per_q = abf::compact_chunks(std::max<uint64_t>(max_bits, ix->n_ads));
     const uint64_t chunks = uint64_t(max_q) * w->chunks_per_q;
+    w->sat_stride = uint32_t((n_words_of(ix->n_ads) + 32u * 32u - 1u) / (32u * 32u));
     abf_status st;
     if ((st = dev_alloc(&w->heavy, max_q)) != ABF_OK || (st = dev_alloc(&w->lpref, max_terms)) != ABF_OK ||
         (st = dev_alloc(&w->tile_cls, max_terms)) != ABF_OK ||
@@ -376,6 +380,7 @@ abf_status ws_alloc(abf_index* ix, uint32_t max_q, uint64_t max_terms, uint64_t 
         (st = dev_alloc(&w->q_dstart, max_q)) != ABF_OK || (st = dev_alloc(&w->q_ndense, max_q)) != ABF_OK ||
         (st = dev_alloc(&w->q_dmode, max_q)) != ABF_OK || (st = dev_alloc(&w->tile_list, max_q)) != ABF_OK ||
         (st = dev_alloc(&w->n_tile_list, 1)) != ABF_OK ||
+        (st = dev_alloc(&w->sat, uint64_t(max_q) * w->sat_stride)) != ABF_OK ||
         (st = dev_alloc(&w->q_terms, max_terms)) != ABF_OK || (st = dev_alloc(&w->q_off, 2)) != ABF_OK) {
         ws_release(w);
         return st;
@@ -537,6 +542,9 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
         }
     }
     ta.skip_dense_only = group ? 1 : 0;
+    // the group kernel marks each (query, tile) it leaves all ones; the
+    // scatter then skips ORs into those tiles
+    if (group) CUDA_TRY(cudaMemsetAsync(ws->sat, 0, uint64_t(b->n_queries) * ws->sat_stride * 4u, s));
     // one launch per window of at most kGroupMaxQueries queries (their
     // per-query state must fit the kernel's shared memory)
     for (uint32_t q0 = 0; group && q0 < b->n_queries; q0 += abf::kGroupMaxQueries) {
@@ -555,6 +563,8 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
         ga.n_words = n_words;
         ga.err = ws->err;
         ga.spin_limit = ws->spin_limit;
+        ga.sat = ws->sat + uint64_t(q0) * ws->sat_stride;
+        ga.sat_stride = ws->sat_stride;
         TIMED(K_GROUP, abf::launch_dense_group(ix->dense_tmap, gw, ga, ix->sm_count, s));
     }
     TIMED(K_TILE, abf::launch_tile_union(v, ta, tt, ix->sm_count, s));
@@ -567,6 +577,11 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
     sa.out = b->d_bitmaps;
     sa.out_stride = b->bitmap_stride_words;
     sa.blocks_per_warp = std::max<uint32_t>(1u, t.scatter_blocks_per_warp);
+    if (group) {
+        sa.sat = ws->sat;
+        sa.sat_stride = ws->sat_stride;
+        sa.sat_shift = gw == 64u ? 6u : 5u;
+    }
     TIMED(K_SCATTER, abf::launch_scatter(v, sa, t, ix->sm_count, s));
     if (maybe_probe) {
         abf::ProbeArgs pr{};

@@ -132,16 +132,29 @@ __device__ __forceinline__ void or_tile(uint32_t* tile, uint32_t lo, uint32_t sp
 }
 
 // OR decoded ids (< n_ads) into a global bitmap, same lane-local combining.
-__device__ __forceinline__ void or_global(uint32_t* bm, uint32_t n_ads, const uint32_t (&id)[4], uint32_t cnt) {
+// true when word wd lies in a tile whose bits are all set already
+__device__ __forceinline__ bool in_full_tile(const uint32_t* sat, uint32_t sat_shift, uint32_t wd) {
+    const uint32_t t = wd >> sat_shift;
+    return (__ldg(sat + (t >> 5)) >> (t & 31u)) & 1u;
+}
+
+// OR of this lane's four ids into the bitmap, one atomic per distinct word;
+// with sat (the dense group kernel's saturated-tile bits of this bitmap),
+// words inside an all-ones tile are skipped: the OR cannot change them
+__device__ __forceinline__ void or_global(uint32_t* bm, uint32_t n_ads, const uint32_t (&id)[4], uint32_t cnt,
+                                          const uint32_t* sat = nullptr, uint32_t sat_shift = 0) {
     const uint32_t lane = lane_id();
     uint32_t cur = kFull, m = 0;
+    auto flush = [&]() {
+        if (!sat || !in_full_tile(sat, sat_shift, cur)) atomicOr(bm + cur, m);
+    };
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const uint32_t i = lane * 4u + k;
         if (i < cnt && id[k] < n_ads) {
             const uint32_t wd = id[k] >> 5, bit = 1u << (id[k] & 31u);
             if (wd != cur) {
-                if (cur != kFull) atomicOr(bm + cur, m);
+                if (cur != kFull) flush();
                 cur = wd;
                 m = bit;
             } else {
@@ -149,7 +162,7 @@ __device__ __forceinline__ void or_global(uint32_t* bm, uint32_t n_ads, const ui
             }
         }
     }
-    if (cur != kFull) atomicOr(bm + cur, m);
+    if (cur != kFull) flush();
 }
 
 template <int NT>
@@ -488,7 +501,10 @@ __device__ __forceinline__ void dense_only_tile(const IndexView& ix, const uint1
                 for (uint32_t e = 0; e < KT; ++e) {
                     acc.x |= x[e].x; acc.y |= x[e].y; acc.z |= x[e].z; acc.w |= x[e].w;
                 }
+                // lists come longest first: a saturated slice reads no more rows
+                if ((acc.x & acc.y & acc.z & acc.w) == ~0u) break;
             }
+            if ((acc.x & acc.y & acc.z & acc.w) == ~0u) k = nd;
             for (; k < nd; ++k) {
                 const uint4 x = __ldg(base + uint64_t(__ldg(dl + k)) * st4 + j);
                 acc.x |= x.x; acc.y |= x.y; acc.z |= x.z; acc.w |= x.w;
@@ -698,6 +714,11 @@ __device__ __forceinline__ uint2 orw(uint2 a, uint2 b) { return make_uint2(a.x |
 template <typename T> __device__ __forceinline__ T zero_word();
 template <> __device__ __forceinline__ uint32_t zero_word<uint32_t>() { return 0u; }
 template <> __device__ __forceinline__ uint2 zero_word<uint2>() { return make_uint2(0u, 0u); }
+__device__ __forceinline__ bool all_ones(uint32_t a) { return a == ~0u; }
+__device__ __forceinline__ bool all_ones(uint2 a) { return (a.x & a.y) == ~0u; }
+// true when the warp's whole tile slice is set: no further row can change it
+template <typename T>
+__device__ __forceinline__ bool tile_full(T acc) { return __all_sync(kFull, all_ones(acc)); }
 
 // Row `woff` (a word offset, row * GW) of a stage, at this lane's column
 // (B = stage + lane * GW / 32 words)
@@ -714,12 +735,18 @@ __device__ __forceinline__ T or8w(const uint8_t* B, uint4 v) {
                    orw(ld_row<T>(B, v.w & 0xffffu), ld_row<T>(B, v.w >> 16))));
 }
 // OR over a list of nd word offsets (padded to a multiple of 8 with the
-// zero row), 16 at a time: per row one extract, one address, one shared load
+// zero row), 16 at a time: per row one extract, one address, one shared load.
+// The lists are in ascending bitmap order, which is longest list first, so a
+// tile of a dense query saturates early; the warp stops once every bit of
+// its slice is set (about 30 % of the row reads on config c1).
 template <typename T>
 __device__ __forceinline__ T or_list_words(const uint8_t* B, const uint4* ol, uint32_t nd) {
     T acc = zero_word<T>();
     uint32_t k = 0;
-    for (; k + 16u <= nd; k += 16u) acc = orw(acc, orw(or8w<T>(B, ol[k >> 3]), or8w<T>(B, ol[(k >> 3) + 1])));
+    for (; k + 16u <= nd; k += 16u) {
+        acc = orw(acc, orw(or8w<T>(B, ol[k >> 3]), or8w<T>(B, ol[(k >> 3) + 1])));
+        if (tile_full(acc)) return acc;
+    }
     if (k < nd) acc = orw(acc, or8w<T>(B, ol[k >> 3]));
     if (k + 8u < nd) acc = orw(acc, or8w<T>(B, ol[(k >> 3) + 1]));
     return acc;
@@ -736,6 +763,7 @@ __device__ __forceinline__ T or_list_rows(const uint8_t* B, const uint4* dl, uin
                                     (v.z & 0xffffu) * GW | ((v.z >> 16) * GW) << 16,
                                     (v.w & 0xffffu) * GW | ((v.w >> 16) * GW) << 16);
         acc = orw(acc, or8w<T>(B, wv));
+        if (tile_full(acc)) break;
     }
     return acc;
 }
@@ -864,6 +892,8 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
                                   : or_list_rows<GW, T>(B, reinterpret_cast<const uint4*>(a.q_dense16 + a.q_dstart[q]),
                                                         nd);
             uint32_t* o = a.out + uint64_t(q) * a.out_stride + w;
+            if (a.sat && tile_full(acc) && lane == 0)
+                atomicOr(a.sat + uint64_t(q) * a.sat_stride + (t >> 5), 1u << (t & 31u));
             if constexpr (GW == 64u) {
                 if (w + 1u < a.n_words) *reinterpret_cast<uint2*>(o) = acc;  // 8-byte aligned (checked at launch)
                 else if (w < a.n_words) o[0] = acc.x;
@@ -912,6 +942,7 @@ __global__ void __launch_bounds__(NW * 32) scatter_kernel(IndexView ix, ScatterA
         uint64_t i = i0;
         uint32_t j = r - a.term_lpref[i];
         uint32_t* out = a.out + uint64_t(a.out_slot ? a.out_slot[q] : q) * a.out_stride;
+        const uint32_t* sat = a.sat ? a.sat + uint64_t(q) * a.sat_stride : nullptr;
         // (i, j) is a scattered block of query q; the walk moves to the next
         // one, crossing into later terms and queries as they run out
         auto advance = [&]() {
@@ -930,22 +961,26 @@ __global__ void __launch_bounds__(NW * 32) scatter_kernel(IndexView ix, ScatterA
                     qtot = uint32_t(a.q_light_pref[q + 1] - a.q_light_pref[q]);
                     i = qb;
                     out = a.out + uint64_t(a.out_slot ? a.out_slot[q] : q) * a.out_stride;
+                    if (a.sat) sat = a.sat + uint64_t(q) * a.sat_stride;
                 }
             }
         };
         Fetched nxt = fetch_block(ix, __ldg(ix.term_blk + a.terms[i]) + j);
         uint32_t* nxt_out = out;
+        const uint32_t* nxt_sat = sat;
         for (uint64_t f = f0; f < f1; ++f) {
             const Fetched cur = nxt;
             uint32_t* cur_out = nxt_out;
+            const uint32_t* cur_sat = nxt_sat;
             if (f + 1 < f1) {  // next block's loads in flight during this decode
                 advance();
                 nxt = fetch_block(ix, __ldg(ix.term_blk + a.terms[i]) + j);
                 nxt_out = out;
+                nxt_sat = sat;
             }
             uint32_t id[4], cnt;
             decode_fetched(cur, stage[warp], id, cnt);
-            or_global(cur_out, ix.n_ads, id, cnt);
+            or_global(cur_out, ix.n_ads, id, cnt, cur_sat, a.sat_shift);
         }
     }
 }
@@ -1148,29 +1183,49 @@ constexpr uint32_t kIdBuf = 1024 + 8;  // one unit's ids plus the 16-byte alignm
 
 // Ids of one unit into dst[0 .. tot): lane l holds word l of the unit in v
 // and the ids of the lower lanes' words in ex; id0 = first id of the unit +
-// lane. Dense units walk all 32 words without bookkeeping; sparse ones
-// visit only the non-zero words. (Two words per shuffle pair, 16 lanes per
-// word, measured 7 % faster on uniformly random 75 %-dense bitmaps but no
-// faster on the c1 bitmaps, where saturated words put both half-warps'
-// stores on the same banks.)
-template <bool kDense, typename Store>
-__device__ __forceinline__ void expand_unit(uint32_t v, uint32_t ex, uint32_t id0, uint32_t lt, uint32_t mybit,
-                                            Store store) {
-    if (kDense) {
-#pragma unroll 8
-        for (uint32_t w = 0; w < 32u; ++w) {
-            const uint32_t word = __shfl_sync(kFull, v, w);
-            const uint32_t pos = __shfl_sync(kFull, ex, w);
-            if (word & mybit) store(pos + __popc(word & lt), id0 + w * 32u);
-        }
-    } else {
-        uint32_t nz = __ballot_sync(kFull, v != 0u);
-        while (nz) {
-            const uint32_t w = __ffs(nz) - 1u;
-            nz &= nz - 1u;
-            const uint32_t word = __shfl_sync(kFull, v, w);
-            const uint32_t pos = __shfl_sync(kFull, ex, w);
-            if (word & mybit) store(pos + __popc(word & lt), id0 + w * 32u);
+// lane. Three expansions, by the unit's id count t:
+//  * t >= kPairMin: two bits per lane -- lanes 0-15 take bits 2j, 2j+1 of
+//    the even word, lanes 16-31 those of the odd word, so one pair of
+//    shuffles serves two words; a lane stores at most two ids per step.
+//  * t < kPairMin: each lane writes the ids of its own word, lowest bit
+//    first, for as many steps as the fullest word of the unit has bits;
+//    no shuffles, and a sparse unit costs steps in proportion to its bits.
+//  * t == 1024 (every bit set) is handled by the caller without bit work.
+// Measured on bitmaps with the per-query densities of config c1: 6 % less
+// time than one lane per bit for every dense unit and a shuffle loop over
+// the non-zero words for the rest, and 2x at 25 % density.
+constexpr uint32_t kPairMin = 384;
+
+template <typename Store>
+__device__ __forceinline__ void expand_pairs(uint32_t v, uint32_t ex, uint32_t id0, Store store) {
+    const uint32_t lane = lane_id();
+    const uint32_t half = lane >> 4, j = lane & 15u;
+    const uint32_t below = (1u << (2u * j)) - 1u;               // bits under this lane's pair
+    const uint32_t base = id0 - lane + half * 32u + 2u * j;     // id of bit 2j of word `half`
+#pragma unroll 4
+    for (uint32_t i = 0; i < 16u; ++i) {
+        const uint32_t w = 2u * i + half;
+        const uint32_t word = __shfl_sync(kFull, v, w);
+        const uint32_t pos = __shfl_sync(kFull, ex, w);
+        const uint32_t b2 = (word >> (2u * j)) & 3u;
+        const uint32_t p = pos + __popc(word & below);
+        const uint32_t id = base + i * 64u;
+        if (b2 & 1u) store(p, id);
+        if (b2 & 2u) store(p + (b2 & 1u), id + 1u);
+    }
+}
+
+template <typename Store>
+__device__ __forceinline__ void expand_lane_word(uint32_t v, uint32_t ex, uint32_t id0, Store store) {
+    const uint32_t lane = lane_id();
+    const uint32_t wb = id0 - lane + 32u * lane;  // id of bit 0 of this lane's word
+    const uint32_t steps = __reduce_max_sync(kFull, uint32_t(__popc(v)));
+    uint32_t w = v, p = ex;
+    for (uint32_t i = 0; i < steps; ++i) {
+        if (w) {
+            store(p, wb + uint32_t(__ffs(w)) - 1u);
+            ++p;
+            w &= w - 1u;
         }
     }
 }
@@ -1238,7 +1293,7 @@ __global__ void __launch_bounds__(256, 6) compact_kernel(CompactArgs a) {
             const uint32_t ex = x - cnt;
             const uint32_t id0 = uint32_t((wbase + k * 32u) * 32u) + lane;
             uint32_t* dst = a.ids + o0;
-            if (ids16 && t >= 64 && o0 + t <= a.capacity) {
+            if (ids16 && o0 + t <= a.capacity) {
                 // the unit's ids go to the warp's shared buffer at their
                 // 16-byte-aligned output position; the aligned middle leaves
                 // by one bulk copy, the ragged ends by plain stores
@@ -1247,8 +1302,20 @@ __global__ void __launch_bounds__(256, 6) compact_kernel(CompactArgs a) {
                 if (lane == 0) bulk_wait_read_all();  // the previous unit's copy has read the buffer
                 __syncwarp();
                 auto st = [sb](uint32_t i, uint32_t id) { sb[i] = id; };
-                if (t >= 256u) expand_unit<true>(v[k], ex, id0, lt, mybit, st);
-                else expand_unit<false>(v[k], ex, id0, lt, mybit, st);
+                if (t == 1024u) {
+                    // every bit set: buf[x] = first id of the unit + x - head
+                    const uint32_t b0 = id0 - lane - head;
+                    uint4* b4 = reinterpret_cast<uint4*>(buf);
+#pragma unroll
+                    for (uint32_t m = lane; m < kIdBuf / 4u; m += 32u) {
+                        const uint32_t x = b0 + 4u * m;
+                        b4[m] = make_uint4(x, x + 1u, x + 2u, x + 3u);
+                    }
+                } else if (t >= kPairMin) {
+                    expand_pairs(v[k], ex, id0, st);
+                } else {
+                    expand_lane_word(v[k], ex, id0, st);
+                }
                 fence_proxy_async();  // these shared writes before the async-proxy read
                 __syncwarp();
                 const uint32_t end = head + t;
@@ -1258,15 +1325,15 @@ __global__ void __launch_bounds__(256, 6) compact_kernel(CompactArgs a) {
                     bulk_s2g(gbase + 4, buf + 4, (mid_hi - 4u) * 4u);
                     bulk_commit();
                 }
-                if (lane >= head && lane < 4u) gbase[lane] = buf[lane];
-                if (mid_hi + lane < end) gbase[mid_hi + lane] = buf[mid_hi + lane];
+                if (lane >= head && lane < 4u && lane < end) gbase[lane] = buf[lane];
+                if (mid_hi + lane < end && mid_hi + lane >= 4u) gbase[mid_hi + lane] = buf[mid_hi + lane];
             } else if (o0 + t <= a.capacity) {  // whole unit fits: no per-id check
-                expand_unit<false>(v[k], ex, id0, lt, mybit, [dst](uint32_t i, uint32_t id) { dst[i] = id; });
+                expand_lane_word(v[k], ex, id0, [dst](uint32_t i, uint32_t id) { dst[i] = id; });
             } else {
                 const uint64_t cap = a.capacity;
                 const uint64_t ob = o0;
                 uint32_t* ids = a.ids;
-                expand_unit<false>(v[k], ex, id0, lt, mybit, [=](uint32_t i, uint32_t id) {
+                expand_lane_word(v[k], ex, id0, [=](uint32_t i, uint32_t id) {
                     if (ob + i < cap) ids[ob + i] = id;
                 });
             }

@@ -146,6 +146,8 @@ struct DenseGroupArgs {
     uint64_t n_words;
     uint32_t* err;
     uint32_t spin_limit;       // polls of an mbarrier wait before it gives up
+    uint32_t* sat;             // optional, zeroed before launch: bit t of query q's sat_stride words
+    uint32_t sat_stride;       //   is set when tile t of its bitmap came out all ones
 };
 
 struct ScatterArgs {
@@ -158,6 +160,9 @@ struct ScatterArgs {
     uint32_t* out;
     uint64_t out_stride;
     uint32_t blocks_per_warp;
+    const uint32_t* sat;       // optional: the dense group kernel's saturated-tile bits
+    uint32_t sat_stride;       //   (words per query); an OR into a word of such a tile
+    uint32_t sat_shift;        //   is skipped; tile = word >> sat_shift
 };
 
 struct ProbeArgs {

@@ -345,7 +345,7 @@ def test_batch_sparse_with_qidx(small):
 
 
 @pytest.mark.parametrize("n_bits", [1, 31, 32, 33, 1000, 65536 + 7, 3 * 65536 * 32 + 5])
-@pytest.mark.parametrize("density", [0.0, 0.01, 0.5, 1.0])
+@pytest.mark.parametrize("density", [0.0, 0.01, 0.3, 0.5, 0.9, 1.0])
 def test_collect_ids(small, n_bits, density):
     torch = _torch()
     rng = np.random.default_rng(n_bits)
@@ -367,6 +367,12 @@ def test_collect_ids(small, n_bits, density):
         torch.cuda.synchronize()
         assert int(d_cnt.item()) == e.size
         assert np.array_equal(small_cap.cpu().numpy().view(np.uint32), e[:e.size // 2])
+        # an id array that is not 16-byte aligned takes the plain-store path
+        odd = torch.empty(cap + 1, dtype=torch.int32, device="cuda")[1:]
+        ab.CollectIdsFromBitmap(small["ix"], d_bm, n_bits, odd, d_cnt)
+        torch.cuda.synchronize()
+        assert int(d_cnt.item()) == e.size
+        assert np.array_equal(odd[:e.size].cpu().numpy().view(np.uint32), e)
 
 
 def test_edge_lists(dev):

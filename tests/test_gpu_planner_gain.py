@@ -1,0 +1,193 @@
+"""What the trained planner gains over the method without it.
+
+A serving-shaped workload -- c4's term counts (lognormal, median 40,
+sigma 2) on a mid-size index, answered in batches of 32 queries -- where the
+paths win on different queries:
+
+  1. labels: each training query's device time on PROBE, UNION and HYBRID,
+     measured by the kernels themselves (alone through abf_batch_run with
+     CUDA events, then rescaled so that each batch of 32's labels add up to
+     the measured batch time of that path);
+  2. training: the MLP fitted with the library's own gradient and Adam
+     kernels (abf_mlp_grad / abf_mlp_adam);
+  3. the method without it, the fixed rule: probe threshold tau from the
+     crossover of the reference's own kernels on this index
+     (oracle/ref_tau.py), HYBRID when a list is as dense as a bucket the
+     reference stores as a bitset;
+  4. evaluation on fresh queries, batch after batch, device-timed: the
+     planner (its fused kernel inside abf_batch_run), the fixed rule, and
+     every constant path.
+
+Asserted, with the margin MARGIN for run-to-run noise: the planner's total
+time is at most (1 + MARGIN) times the fixed rule's and the best constant
+path's, and its results are bit-exact. In batches of 32, UNION is the
+fastest path for nearly every query, so the planner's choices are close to
+constant there; the second test takes the same queries one at a time, where
+HYBRID wins for a fifth of them, and asserts that a planner trained on the
+isolated labels picks more than one path and costs, by those labels, at most
+(1 + MARGIN) times the best constant path and no more than the fixed rule.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import adabool_b200 as ab
+from adabool_b200 import Index, planner as P, workload as W
+from adabool_b200 import _native as N
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+MARGIN = 0.05
+BATCH = 32
+SPEC = W.ListsSpec(n_terms=1 << 18, n_ads=1 << 22, nnz=60_000_000, zipf_s=1.05, max_len=1_250_000, seed=13)
+QUERIES = dict(kind="lognormal", median=40.0, sigma=2.0, lo=1, hi=20000)
+N_TRAIN, N_EVAL = 6144, 2048
+N_EVAL_ALONE = 1024
+# features 12 and 13 are the query's position in its batch over the batch
+# size and log1p(batch size); the rest depend on the query alone
+ALONE_FEATURES = {12: 0.0, 13: float(np.log1p(1.0))}
+
+
+def _time_batches(ix, ws, qoff, qt, path, reps=3):
+    """Device time (ms) of answering every batch of BATCH queries, one
+    abf_batch_run per batch on one stream, best of `reps` passes."""
+    import torch
+    dt, do = P.device_batch(qoff, qt)
+    stride = (ix.n_words + 3) // 4 * 4
+    bms = torch.empty((BATCH, stride), dtype=torch.int32, device="cuda")
+    s = torch.cuda.Stream()
+    L = ab.lib()
+    n = qoff.size - 1
+
+    def run_all():
+        for a in range(0, n, BATCH):
+            b = min(n, a + BATCH)
+            bt = N.Batch(N.ptr(dt), C.c_void_p(do.data_ptr() + 8 * a), b - a, None, path, N.ptr(bms), stride, None, 0,
+                         None)
+            N.check(L.abf_batch_run(ix.handle, ws.handle, C.byref(bt), N.stream_ptr(s)))
+
+    run_all()
+    s.synchronize()
+    best = float("inf")
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        run_all()
+        e1.record(s)
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    ws.check(s)
+    return best
+
+
+def _features_in_batches(ix, qoff, qt):
+    out = []
+    for a in range(0, qoff.size - 1, BATCH):
+        b = min(qoff.size - 1, a + BATCH)
+        out.append(P.features(ix, (qoff[a:b + 1] - qoff[a]).astype(np.uint64), qt[qoff[a]:qoff[b]]))
+    return np.concatenate(out)
+
+
+@pytest.fixture(scope="module")
+def setup(dev):
+    off, ads = W.gen_lists(SPEC)
+    lens = np.diff(off).astype(np.uint32)
+    ix = Index.from_csr(off, ads, SPEC.n_terms, SPEC.n_ads, device=0)
+    ix.set_tuning(heavy_min_len=max(128, SPEC.n_ads // 1024), probe_cap=BATCH)
+    tr = W.gen_queries(W.QueriesSpec(N_TRAIN, seed=101, **QUERIES), lens)
+    ev = W.gen_queries(W.QueriesSpec(N_EVAL, seed=202, **QUERIES), lens)
+    # kernel-timed labels of every training query run alone
+    iso = P.collect_labels(ix, *tr)
+    # the fixed rule's probe threshold from the reference's kernels
+    from oracle import ref_tau as RT
+    frac = P.touched_fraction(ix, *ev)
+    rt = RT.reference_tau(off, ads, SPEC.n_terms, SPEC.n_ads, ev[0], ev[1], frac)
+    assert "tau" in rt, rt
+    return dict(off=off, ads=ads, lens=lens, ix=ix, tr=tr, ev=ev, iso=iso, rt=rt)
+
+
+def test_trained_planner_beats_fixed_rule_and_constants(setup):
+    import torch
+    ix = setup["ix"]
+    tr_off, tr_t = setup["tr"]
+    ev_off, ev_t = setup["ev"]
+    rt = setup["rt"]
+    # 1-2: kernel-timed labels in batches of BATCH, training on the GPU
+    lab = P.collect_labels_batched(ix, tr_off, tr_t, setup["iso"], group=BATCH)
+    fit = P.train(_features_in_batches(ix, tr_off, tr_t), np.log(lab), epochs=150, batch=4096, lr=2e-3)
+    # 3: the fixed rule from the reference's kernels
+    ix.set_tuning(probe_min_fraction=rt["tau"])
+    # 4: evaluation, batch after batch
+    ws = ix.workspace(BATCH, int(np.diff(ev_off).max()) * BATCH + 1)
+    times = {name: _time_batches(ix, ws, ev_off, ev_t, p)
+             for name, p in (("probe", ab.PATH_PROBE), ("union", ab.PATH_UNION), ("hybrid", ab.PATH_HYBRID))}
+    times["fixed_rule"] = _time_batches(ix, ws, ev_off, ev_t, ab.PATH_AUTO)
+    P.install(ix, fit.params)
+    try:
+        times["planner"] = _time_batches(ix, ws, ev_off, ev_t, ab.PATH_AUTO)
+        choices = []
+        for a in range(0, ev_off.size - 1, BATCH):
+            b = min(ev_off.size - 1, a + BATCH)
+            dt, do = P.device_batch((ev_off[a:b + 1] - ev_off[a]).astype(np.uint64), ev_t[ev_off[a]:ev_off[b]])
+            paths = torch.zeros(b - a, dtype=torch.uint8, device="cuda")
+            N.check(ab.lib().abf_planner_predict(ix.handle, N.ptr(dt), N.ptr(do), b - a, None, N.ptr(paths), None))
+            choices.append(paths.cpu().numpy())
+        choices = np.concatenate(choices)
+        # bit-exact on a sample of batches
+        stride = (ix.n_words + 3) // 4 * 4
+        for a in range(0, ev_off.size - 1, 16 * BATCH):
+            b = min(ev_off.size - 1, a + BATCH)
+            qo = (ev_off[a:b + 1] - ev_off[a]).astype(np.uint64)
+            qt = ev_t[ev_off[a]:ev_off[b]]
+            dt, do = P.device_batch(qo, qt)
+            bms = torch.empty((b - a, stride), dtype=torch.int32, device="cuda")
+            ix.batch_run(ws, dt, do, b - a, bms, stride, path=ab.PATH_AUTO)
+            got = bms.cpu().numpy().view(np.uint32)
+            for i in range(b - a):
+                e = O.kway_union(setup["off"], setup["ads"], qt[qo[i]:qo[i + 1]])
+                assert np.array_equal(got[i, :ix.n_words], O.ids_to_bitmap(e, ix.n_words)), (a + i)
+    finally:
+        P.uninstall(ix)
+    share = {N.PATH_NAMES[int(p)]: int((choices == p).sum()) for p in np.unique(choices)}
+    best_const = min(times["probe"], times["union"], times["hybrid"])
+    print(f"\nbatch times (ms): {times}; planner choices {share}; reference tau {rt}; val mse {fit.val_loss:.4f}")
+    assert times["planner"] <= (1 + MARGIN) * times["fixed_rule"], times
+    assert times["planner"] <= (1 + MARGIN) * best_const, times
+
+
+def _alone(X):
+    X = X.copy()
+    for j, v in ALONE_FEATURES.items():
+        X[:, j] = v
+    return X
+
+
+def test_planner_picks_per_query_paths_alone(setup):
+    """Queries one at a time: the planner trained on the isolated labels
+    against the constant paths and the fixed rule, by the measured labels of
+    fresh queries."""
+    ix = setup["ix"]
+    tr_off, tr_t = setup["tr"]
+    ev_off, ev_t = setup["ev"]
+    fit = P.train(_alone(P.features(ix, tr_off, tr_t)), np.log(setup["iso"]), epochs=150, batch=4096, lr=2e-3)
+    n = N_EVAL_ALONE
+    eo, et = ev_off[:n + 1], ev_t[:ev_off[n]]
+    lab = P.collect_labels(ix, eo, et)
+    choice = P.mlp_predict(fit.params, _alone(P.features(ix, eo, et))).argmin(1)
+    fixed = P.fixed_rule_choice(ix, eo, et, setup["rt"]["tau"], int(ix.tuning.fixed_hybrid_min_len))
+    rows = np.arange(n)
+    cost = {"planner": float(lab[rows, choice].sum()), "fixed_rule": float(lab[rows, fixed].sum()),
+            "best": float(lab.min(1).sum())}
+    for j, p in enumerate(P.PATHS):
+        cost[N.PATH_NAMES[int(p)]] = float(lab[:, j].sum())
+    best_const = min(lab.sum(0))
+    picked = {N.PATH_NAMES[int(P.PATHS[j])]: int((choice == j).sum()) for j in np.unique(choice)}
+    best_share = {N.PATH_NAMES[int(P.PATHS[j])]: int((lab.argmin(1) == j).sum()) for j in np.unique(lab.argmin(1))}
+    agree = float((choice == lab.argmin(1)).mean())
+    print(f"\nalone, label us: {cost}; planner picks {picked}; best path {best_share}; agreement {agree:.3f}; "
+          f"val mse {fit.val_loss:.4f}")
+    assert len(picked) >= 2, f"the planner picks one path for every query: {picked}"
+    assert cost["planner"] <= (1 + MARGIN) * best_const, cost
+    assert cost["planner"] <= cost["fixed_rule"], cost
