@@ -1279,11 +1279,19 @@ __global__ void __launch_bounds__(256, 6) compact_kernel(CompactArgs a) {
         }
         __syncthreads();
         uint64_t o0 = s_prefix + __reduce_add_sync(kFull, lane < warp ? s_wtot[lane] : 0u);
-#pragma unroll
+#pragma unroll 1
         for (uint32_t k = 0; k < kWarpUnits; ++k) {
-            const uint32_t t = tot[k];
+            // a rolled loop keeps one copy of the expansion code (the
+            // instruction cache holds it): the current unit is always in
+            // v[0], the later ones move down one register per step
+            const uint32_t vk = v[0], t = tot[0];
+#pragma unroll
+            for (uint32_t j = 0; j + 1 < kWarpUnits; ++j) {
+                v[j] = v[j + 1];
+                tot[j] = tot[j + 1];
+            }
             if (t == 0) continue;
-            const uint32_t cnt = __popc(v[k]);
+            const uint32_t cnt = __popc(vk);
             uint32_t x = cnt;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -1312,9 +1320,9 @@ __global__ void __launch_bounds__(256, 6) compact_kernel(CompactArgs a) {
                         b4[m] = make_uint4(x, x + 1u, x + 2u, x + 3u);
                     }
                 } else if (t >= kPairMin) {
-                    expand_pairs(v[k], ex, id0, st);
+                    expand_pairs(vk, ex, id0, st);
                 } else {
-                    expand_lane_word(v[k], ex, id0, st);
+                    expand_lane_word(vk, ex, id0, st);
                 }
                 fence_proxy_async();  // these shared writes before the async-proxy read
                 __syncwarp();
@@ -1328,12 +1336,12 @@ __global__ void __launch_bounds__(256, 6) compact_kernel(CompactArgs a) {
                 if (lane >= head && lane < 4u && lane < end) gbase[lane] = buf[lane];
                 if (mid_hi + lane < end && mid_hi + lane >= 4u) gbase[mid_hi + lane] = buf[mid_hi + lane];
             } else if (o0 + t <= a.capacity) {  // whole unit fits: no per-id check
-                expand_lane_word(v[k], ex, id0, [dst](uint32_t i, uint32_t id) { dst[i] = id; });
+                expand_lane_word(vk, ex, id0, [dst](uint32_t i, uint32_t id) { dst[i] = id; });
             } else {
                 const uint64_t cap = a.capacity;
                 const uint64_t ob = o0;
                 uint32_t* ids = a.ids;
-                expand_lane_word(v[k], ex, id0, [=](uint32_t i, uint32_t id) {
+                expand_lane_word(vk, ex, id0, [=](uint32_t i, uint32_t id) {
                     if (ob + i < cap) ids[ob + i] = id;
                 });
             }
