@@ -1160,8 +1160,8 @@ __device__ bool lookback_prefix(uint64_t* status, uint64_t item, uint32_t agg, u
 // each store instruction writes one contiguous run and no lane loops over
 // bits. The bitmap is read once: there is no separate counting pass.
 constexpr uint32_t kUnits = kCompactChunkWords / 32;
-constexpr uint32_t kWarpUnits = kUnits / 8;
-static_assert(kUnits == 64, "8 warps x 8 units cover one chunk");
+constexpr uint32_t kWarpUnits = kUnits / kCompactWarps;
+static_assert(kWarpUnits == 8, "each warp covers 8 units of its CTA's chunk");
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
@@ -1230,9 +1230,9 @@ __device__ __forceinline__ void expand_lane_word(uint32_t v, uint32_t ex, uint32
     }
 }
 
-__global__ void __launch_bounds__(256, 6) compact_kernel(CompactArgs a) {
-    __shared__ __align__(16) uint32_t s_buf[8][kIdBuf];
-    __shared__ uint32_t s_wtot[8];
+__global__ void __launch_bounds__(kCompactWarps * 32, 48 / kCompactWarps) compact_kernel(CompactArgs a) {
+    __shared__ __align__(16) uint32_t s_buf[kCompactWarps][kIdBuf];
+    __shared__ uint32_t s_wtot[kCompactWarps];
     __shared__ unsigned long long s_item, s_prefix;
     const uint32_t lane = lane_id(), warp = warp_id();
     const uint32_t lt = lanemask_lt(), mybit = 1u << lane;
@@ -1264,7 +1264,7 @@ __global__ void __launch_bounds__(256, 6) compact_kernel(CompactArgs a) {
         if (lane == 0) s_wtot[warp] = wsum;
         __syncthreads();
         if (warp == 0) {
-            const uint32_t t = __reduce_add_sync(kFull, lane < 8u ? s_wtot[lane] : 0u);
+            const uint32_t t = __reduce_add_sync(kFull, lane < kCompactWarps ? s_wtot[lane] : 0u);
             uint64_t excl = 0;
             const bool ok = lookback_prefix(a.status, item, t, a.spin_limit, &excl);
             if (lane == 0) {
@@ -1589,7 +1589,9 @@ cudaError_t launch_compact(const CompactArgs& a, int sm_count, uint32_t ctas_per
     if (e == cudaSuccess) e = cudaMemsetAsync(a.ticket, 0, sizeof(unsigned long long), s);
     if (e == cudaSuccess && a.id_counts) e = cudaMemsetAsync(a.id_counts, 0, uint64_t(a.n_q) * sizeof(uint64_t), s);
     if (e != cudaSuccess) return e;
-    compact_kernel<<<grid_for(items, sm_count, ctas_per_sm ? ctas_per_sm : 6u), 256, 0, s>>>(a);
+    // ctas_per_sm counts CTAs of 8 warps: the same resident warps whatever the CTA size
+    const uint32_t per_sm = (ctas_per_sm ? ctas_per_sm : 6u) * 8u / kCompactWarps;
+    compact_kernel<<<grid_for(items, sm_count, per_sm), kCompactWarps * 32, 0, s>>>(a);
     count_launch();
     return cudaGetLastError();
 }
