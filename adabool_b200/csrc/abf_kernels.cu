@@ -1100,8 +1100,10 @@ __device__ __forceinline__ uint32_t masked_word(const uint32_t* bm, uint64_t w, 
 __device__ __forceinline__ uint64_t ld_status(const uint64_t* p) {
     return *reinterpret_cast<const volatile unsigned long long*>(p);
 }
+// A status word carries its own value, and no other write of a work item is
+// read by another CTA while the kernel runs, so publishing needs no fence:
+// one atomic exchange at L2, where the look-back's volatile loads read it.
 __device__ __forceinline__ void st_status(uint64_t* p, uint64_t v) {
-    __threadfence();
     atomicExch(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(v));
 }
 
@@ -1162,12 +1164,6 @@ __device__ bool lookback_prefix(uint64_t* status, uint64_t item, uint32_t agg, u
 constexpr uint32_t kUnits = kCompactChunkWords / 32;
 constexpr uint32_t kWarpUnits = kUnits / kCompactWarps;
 static_assert(kWarpUnits == 8, "each warp covers 8 units of its CTA's chunk");
-
-__device__ __forceinline__ uint32_t lanemask_lt() {
-    uint32_t m;
-    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-    return m;
-}
 
 // bulk copy shared -> global (TMA engine), completion tracked per thread
 __device__ __forceinline__ void bulk_s2g(void* gdst, const void* ssrc, uint32_t bytes) {
@@ -1235,7 +1231,6 @@ __global__ void __launch_bounds__(kCompactWarps * 32, 48 / kCompactWarps) compac
     __shared__ uint32_t s_wtot[kCompactWarps];
     __shared__ unsigned long long s_item, s_prefix;
     const uint32_t lane = lane_id(), warp = warp_id();
-    const uint32_t lt = lanemask_lt(), mybit = 1u << lane;
     const bool ids16 = (reinterpret_cast<uintptr_t>(a.ids) & 15u) == 0;
     uint32_t* buf = s_buf[warp];
     const uint64_t n_words = (a.n_bits + 31) / 32;

@@ -108,6 +108,28 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def write_only_gbs(dev, gib: int = 4, reps: int = 5) -> float:
+    """Write-only HBM rate of this GPU right now: best of `reps` fills of a
+    `gib` GiB buffer, CUDA events. The compaction's traffic is almost all
+    writes, so this is the ceiling it is also compared with."""
+    import torch
+    n = (gib << 30) // 4
+    x = torch.empty(n, dtype=torch.int32, device=dev)
+    x.fill_(1)
+    torch.cuda.synchronize(dev)
+    best = float("inf")
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        x.fill_(7)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del x
+    torch.cuda.empty_cache()
+    return 4.0 * n / (best / 1e3) / 1e9
+
+
 class ClockSampler:
     """nvidia-smi samples of the SM clock and throttle reasons while running."""
 
@@ -463,6 +485,12 @@ def run_ours(args, rank, world, dev):
                 "traffic_source": None if ratio is None else TRAFFIC_SOURCE.get(dom),
                 "duration_source": "CUDA events around each launch in a single-stream pass of the same steps "
                                    "right after the timed region"}
+        if dom == "compact":
+            wgbs = write_only_gbs(dev)
+            roof["write_only_gbs_live"] = round(wgbs, 1)
+            roof["frac_of_write_only"] = round(a / wgbs, 4)
+            roof["write_note"] = ("the compaction writes 4 bytes per id and reads 1 bit per ad (96 % writes on c1); "
+                                  "write_only_gbs_live is a 4 GiB fill timed on this GPU after the profile pass")
     step_bytes = float(sum(alg.values()))
     postings = float(np.sum(qpost))
     value = n_q * world / (ms_step / 1e3)
