@@ -138,6 +138,24 @@ __device__ __forceinline__ bool in_full_tile(const uint32_t* sat, uint32_t sat_s
     return (__ldg(sat + (t >> 5)) >> (t & 31u)) & 1u;
 }
 
+// true when every tile that ids [lo, hi) can touch is marked all ones
+// (tile = word >> sat_shift): the whole block can be skipped, decode
+// included. Ranges over more than 32 words of marks are not checked.
+__device__ __forceinline__ bool range_saturated(const uint32_t* sat, uint32_t sat_shift, uint32_t lo, uint32_t hi) {
+    const uint32_t t0 = (lo >> 5) >> sat_shift, t1 = ((hi - 1u) >> 5) >> sat_shift;
+    const uint32_t w0 = t0 >> 5, nw = (t1 >> 5) - w0 + 1u;
+    if (nw > 32u) return false;  // warp-uniform
+    const uint32_t lane = lane_id();
+    bool ok = true;
+    if (lane < nw) {
+        uint32_t m = ~0u;
+        if (lane == 0) m &= ~0u << (t0 & 31u);
+        if (lane + 1u == nw) m &= ~0u >> (31u - (t1 & 31u));
+        ok = (__ldg(sat + w0 + lane) & m) == m;
+    }
+    return __all_sync(kFull, ok);
+}
+
 // OR of this lane's four ids into the bitmap, one atomic per distinct word;
 // with sat (the dense group kernel's saturated-tile bits of this bitmap),
 // words inside an all-ones tile are skipped: the OR cannot change them
@@ -965,19 +983,35 @@ __global__ void __launch_bounds__(NW * 32) scatter_kernel(IndexView ix, ScatterA
                 }
             }
         };
-        Fetched nxt = fetch_block(ix, __ldg(ix.term_blk + a.terms[i]) + j);
+        // exclusive bound on the ids of block b, the j-th of slot i: the next
+        // block's first id, or n_ads after the term's last block (only
+        // needed with saturation marks)
+        auto block_hi = [&](uint32_t b) -> uint32_t {
+            if (!a.sat) return ix.n_ads;
+            const uint32_t nb = (i + 1 < qe ? a.term_lpref[i + 1] : qtot) - a.term_lpref[i];
+            return j + 1u < nb ? __ldg(ix.blk_first + b + 1u) : ix.n_ads;
+        };
+        uint32_t b = __ldg(ix.term_blk + a.terms[i]) + j;
+        Fetched nxt = fetch_block(ix, b);
+        uint32_t nxt_hi = block_hi(b);
         uint32_t* nxt_out = out;
         const uint32_t* nxt_sat = sat;
         for (uint64_t f = f0; f < f1; ++f) {
             const Fetched cur = nxt;
+            const uint32_t cur_hi = nxt_hi;
             uint32_t* cur_out = nxt_out;
             const uint32_t* cur_sat = nxt_sat;
             if (f + 1 < f1) {  // next block's loads in flight during this decode
                 advance();
-                nxt = fetch_block(ix, __ldg(ix.term_blk + a.terms[i]) + j);
+                b = __ldg(ix.term_blk + a.terms[i]) + j;
+                nxt = fetch_block(ix, b);
+                nxt_hi = block_hi(b);
                 nxt_out = out;
                 nxt_sat = sat;
             }
+            // a block whose whole id range lies in tiles the dense lists
+            // already filled changes nothing: skip its decode and ORs
+            if (cur_sat && range_saturated(cur_sat, a.sat_shift, cur.first, cur_hi)) continue;
             uint32_t id[4], cnt;
             decode_fetched(cur, stage[warp], id, cnt);
             or_global(cur_out, ix.n_ads, id, cnt, cur_sat, a.sat_shift);
