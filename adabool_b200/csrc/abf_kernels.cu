@@ -1186,15 +1186,13 @@ __device__ bool lookback_prefix(uint64_t* status, uint64_t item, uint32_t agg, u
     return true;
 }
 
-// One CTA per (bitmap, 2048-word chunk) at a time, items taken in ascending
-// order from a ticket counter. Each of the 8 warps owns 8 consecutive units
-// of 32 words, held in registers (lane l: word l of each unit); their
-// popcounts give the chunk's id count, warp 0 looks back for the chunk's
-// output offset, and then every warp expands its units on its own, one word
-// at a time with one lane per bit: the lanes holding set bits store their
-// ids to consecutive output addresses (rank = popcount of the lower bits), so
-// each store instruction writes one contiguous run and no lane loops over
-// bits. The bitmap is read once: there is no separate counting pass.
+// One CTA per (bitmap, 1024-word chunk) at a time, items taken in ascending
+// order from a ticket counter. Each of the 4 warps owns 8 consecutive units
+// of 32 words, held in registers (lane l: word l of each unit); the chunk's
+// id count is published and its output offset found by a decoupled
+// look-back before the CTA starts it, and then every warp expands its units
+// on its own into ascending ids (three expansions by the unit's id count,
+// below). The bitmap is read once: there is no separate counting pass.
 constexpr uint32_t kUnits = kCompactChunkWords / 32;
 constexpr uint32_t kWarpUnits = kUnits / kCompactWarps;
 static_assert(kWarpUnits == 8, "each warp covers 8 units of its CTA's chunk");
@@ -1260,54 +1258,100 @@ __device__ __forceinline__ void expand_lane_word(uint32_t v, uint32_t ex, uint32
     }
 }
 
+// async 4-byte copy global -> shared (LDGSTS: no register round trip)
+__device__ __forceinline__ void cp_async4(void* sdst, const void* gsrc) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(sdst)), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+// One warp claims the next work item and makes it ready for the CTA: the
+// chunk's words into buf (lane l: word 32 m + l), each warp slice's id count
+// into s_wtot, the decoupled look-back's exclusive prefix into *s_prefix.
+// The claim is followed at once by the loads and the count's publication, so
+// later items' look-backs never wait long on it.
+__device__ void prepare_chunk(const CompactArgs& a, uint64_t items, uint64_t n_words, uint32_t* buf,
+                              unsigned long long* s_item, unsigned long long* s_prefix, uint32_t* s_wtot) {
+    const uint32_t lane = lane_id();
+    unsigned long long n = 0;
+    if (lane == 0) n = atomicAdd(a.ticket, 1ull);
+    n = __shfl_sync(kFull, n, 0);
+    if (lane == 0) *s_item = n;
+    if (n >= items) return;
+    const uint32_t q = uint32_t(n / a.n_chunks);
+    const uint32_t c = uint32_t(n - uint64_t(q) * a.n_chunks);
+    const uint32_t* bm = a.bm + uint64_t(q) * a.stride;
+    const uint64_t wbase = uint64_t(c) * kCompactChunkWords;
+#pragma unroll 8
+    for (uint32_t m = 0; m < kUnits; ++m) {
+        const uint64_t wi = wbase + m * 32u + lane;
+        if (wi + 1u < n_words) cp_async4(buf + m * 32u + lane, bm + wi);
+        else buf[m * 32u + lane] = wi < n_words ? masked_word(bm, wi, a.n_bits) : 0u;
+    }
+    cp_async_wait_all();
+    __syncwarp();
+    uint32_t t = 0;
+#pragma unroll
+    for (uint32_t w = 0; w < kCompactWarps; ++w) {
+        uint32_t cw = 0;
+#pragma unroll
+        for (uint32_t k = 0; k < kWarpUnits; ++k) cw += __popc(buf[(w * kWarpUnits + k) * 32u + lane]);
+        cw = __reduce_add_sync(kFull, cw);
+        if (lane == 0) s_wtot[w] = cw;
+        t += cw;
+    }
+    uint64_t excl = 0;
+    const bool ok = lookback_prefix(a.status, n, t, a.spin_limit, &excl);
+    if (lane == 0) {
+        if (!ok) atomicOr(a.err, kErrScanTimeout);
+        *s_prefix = excl;
+        if (a.id_offsets) {
+            if (c == 0) a.id_offsets[q] = excl;
+            if (n + 1 == items) a.id_offsets[a.n_q] = excl + t;
+        }
+        if (a.id_counts && t) atomicAdd(reinterpret_cast<unsigned long long*>(a.id_counts + q), t);
+    }
+}
+
+// The CTA works on one item while the first of its warps to finish prepares
+// the next one in its own id buffer (claim, loads, count, look-back), so the
+// claim's round trip, the loads and the look-back overlap the other warps'
+// expansion instead of stalling the whole CTA.
 __global__ void __launch_bounds__(kCompactWarps * 32, 48 / kCompactWarps) compact_kernel(CompactArgs a) {
     __shared__ __align__(16) uint32_t s_buf[kCompactWarps][kIdBuf];
     __shared__ uint32_t s_wtot[kCompactWarps];
     __shared__ unsigned long long s_item, s_prefix;
+    __shared__ uint32_t s_src, s_first;
+    static_assert(kCompactChunkWords <= kIdBuf, "a chunk fits one id buffer");
     const uint32_t lane = lane_id(), warp = warp_id();
     const bool ids16 = (reinterpret_cast<uintptr_t>(a.ids) & 15u) == 0;
     uint32_t* buf = s_buf[warp];
     const uint64_t n_words = (a.n_bits + 31) / 32;
     const uint64_t items = uint64_t(a.n_q) * a.n_chunks;
+    if (warp == 0) prepare_chunk(a, items, n_words, buf, &s_item, &s_prefix, s_wtot);
+    if (threadIdx.x == 0) {
+        s_src = 0;
+        s_first = 0;
+    }
+    __syncthreads();
     for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(a.ticket, 1ull);
-        __syncthreads();
         const uint64_t item = s_item;
         if (item >= items) break;
         const uint32_t q = uint32_t(item / a.n_chunks);
         const uint32_t c = uint32_t(item - uint64_t(q) * a.n_chunks);
-        const uint32_t* bm = a.bm + uint64_t(q) * a.stride;
         const uint64_t wbase = uint64_t(c) * kCompactChunkWords + uint64_t(warp) * (kWarpUnits * 32u);
+        const uint32_t* src = s_buf[s_src] + warp * (kWarpUnits * 32u);
         uint32_t v[kWarpUnits], tot[kWarpUnits];
 #pragma unroll
         for (uint32_t k = 0; k < kWarpUnits; ++k) {
-            const uint64_t wi = wbase + k * 32u + lane;
-            v[k] = wi < n_words ? masked_word(bm, wi, a.n_bits) : 0u;
-        }
-        uint32_t wsum = 0;
-#pragma unroll
-        for (uint32_t k = 0; k < kWarpUnits; ++k) {
+            v[k] = src[k * 32u + lane];
             tot[k] = __reduce_add_sync(kFull, uint32_t(__popc(v[k])));
-            wsum += tot[k];
         }
-        if (lane == 0) s_wtot[warp] = wsum;
-        __syncthreads();
-        if (warp == 0) {
-            const uint32_t t = __reduce_add_sync(kFull, lane < kCompactWarps ? s_wtot[lane] : 0u);
-            uint64_t excl = 0;
-            const bool ok = lookback_prefix(a.status, item, t, a.spin_limit, &excl);
-            if (lane == 0) {
-                if (!ok) atomicOr(a.err, kErrScanTimeout);
-                s_prefix = excl;
-                if (a.id_offsets) {
-                    if (c == 0) a.id_offsets[q] = excl;
-                    if (item + 1 == items) a.id_offsets[a.n_q] = excl + t;
-                }
-                if (a.id_counts && t) atomicAdd(reinterpret_cast<unsigned long long*>(a.id_counts + q), t);
-            }
-        }
-        __syncthreads();
         uint64_t o0 = s_prefix + __reduce_add_sync(kFull, lane < warp ? s_wtot[lane] : 0u);
+        // every warp holds its words and offset: the chunk's buffer and the
+        // next item's slots may be reused
+        __syncthreads();
 #pragma unroll 1
         for (uint32_t k = 0; k < kWarpUnits; ++k) {
             // a rolled loop keeps one copy of the expansion code (the
@@ -1376,6 +1420,18 @@ __global__ void __launch_bounds__(kCompactWarps * 32, 48 / kCompactWarps) compac
             }
             o0 += t;
         }
+        // the first warp done prepares the next item in its own buffer
+        uint32_t first = 0;
+        if (lane == 0) first = atomicAdd(&s_first, 1u);
+        first = __shfl_sync(kFull, first, 0);
+        if (first == 0) {
+            if (lane == 0) bulk_wait_read_all();  // its last copy has read the buffer
+            __syncwarp();
+            prepare_chunk(a, items, n_words, buf, &s_item, &s_prefix, s_wtot);
+            if (lane == 0) s_src = warp;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_first = 0;
     }
     if (lane == 0) bulk_wait_all();
 }

@@ -31,9 +31,9 @@ namespace abf {
 
 constexpr uint32_t kNoHeavy = 0xffffffffu;   // heavy_min meaning "merge no list"
 constexpr uint32_t kDenseOnly = 0xfffffffeu; // heavy_min meaning "merge only the dense-bitmap lists"
-// warps per compaction CTA (4 and 2 measured the same on c1: 19.30 and
-// 19.54 ms per step against 19.43)
-constexpr uint32_t kCompactWarps = 8;
+// warps per compaction CTA; a chunk (256 words per warp) fits one warp's id
+// buffer, where the warp that prepares it stages it
+constexpr uint32_t kCompactWarps = 4;
 constexpr uint32_t kCompactChunkWords = kCompactWarps * 256;  // bitmap words per compaction work item
 constexpr uint32_t kProbeGroup = 32;          // probe queries tested per pass
 

@@ -6,9 +6,9 @@
 // synchronisation would stall the other streams, or code that must not run
 // into out-of-memory in the middle of a request. This entry point uses no
 // cudaMalloc/cudaFree (and no allocating library call): the compaction's
-// scratch -- one look-back status word per 2048-word chunk, the item ticket
+// scratch -- one look-back status word per 1024-word chunk, the item ticket
 // and an error word -- lives in one file-scope device array, sized for
-// bitmaps of at most ABF_NOALLOC_MAX_BITS bits (about 128 KB, held on every
+// bitmaps of at most ABF_NOALLOC_MAX_BITS bits (about 256 KB, held on every
 // device that loads the library until the process exits).
 //
 // Host code may not pass the array's name to a kernel (on the host it is

@@ -264,7 +264,7 @@ abf_status abf_batch_collect_ids(abf_index* index, abf_workspace* ws, const uint
  * to allocate, a serving thread that cannot afford cudaMalloc's possible
  * device-wide synchronisation, code that must not hit out-of-memory in
  * the middle of a request. Needs no index and calls no cudaMalloc/cudaFree:
- * its scratch is one static device array (about 128 KB per device, kept
+ * its scratch is one static device array (about 256 KB per device, kept
  * until the process exits) sized for at most ABF_NOALLOC_MAX_BITS bits.
  * Larger bitmaps are refused with ABF_ERR_CAPACITY -- where abf_collect_ids
  * refuses only bitmaps above 2^32 bits, with ABF_ERR_RANGE. The first call
