@@ -166,8 +166,9 @@ typedef struct abf_tuning {
                                  ceil(33 * n_ads / 256): the density at which the
                                  reference stores a 256-id bucket as a bitset
                                  (src/AdaBool/inverted_list.h:425-458) */
-    uint32_t compact_ctas_per_sm; /* resident CTAs per SM of the compaction (1..6, default
-                                 6); fewer leave room for another stream's kernels */
+    uint32_t compact_ctas_per_sm; /* resident warps per SM of the compaction, in eights
+                                 (1..6, default 6 = 48 warps, 12 CTAs of 4 warps);
+                                 fewer leave room for another stream's kernels */
     uint32_t group_tile_words;  /* dense group kernel tile: 0 = 64 words where a stage and
                                  the window's lists fit shared memory, else 32; 64 = 64
                                  words wherever one stage fits (lists then read from
