@@ -518,12 +518,11 @@ abf_status run_batch(abf_index* ix, abf_workspace* ws, const abf_batch* b, const
     uint32_t gw = 32, stages = 2;
     if (out8 && abf::dense_group_list_cap(n_dense + 1, wq, 64, 2) >= 64u * wq) {
         gw = 64;
-    } else if (out8 && abf::dense_group_list_cap(n_dense + 1, wq, 64, 1) >= 64u * wq) {
-        gw = 64;
-        stages = 1;
-    } else if (out8 && t.group_tile_words == 64 && abf::dense_group_list_cap(n_dense + 1, wq, 64, 1) > 0) {
-        // 64-word tiles asked for where the window's lists do not fit beside
-        // them: one stage, the lists read from global memory
+    } else if (out8 && abf::dense_group_list_cap(n_dense + 1, wq, 64, 1) > 0) {
+        // one 64-word stage wherever it fits: the kernel keeps the window's
+        // lists in shared memory beside it when they fit and reads them from
+        // global memory otherwise; 32-word tiles cost twice the index work
+        // per word (c1, 512-query windows: 5.60 against 7.46 ms per step)
         gw = 64;
         stages = 1;
     }

@@ -169,10 +169,11 @@ typedef struct abf_tuning {
     uint32_t compact_ctas_per_sm; /* resident warps per SM of the compaction, in eights
                                  (1..6, default 6 = 48 warps, 12 CTAs of 4 warps);
                                  fewer leave room for another stream's kernels */
-    uint32_t group_tile_words;  /* dense group kernel tile: 0 = 64 words where a stage and
-                                 the window's lists fit shared memory, else 32; 64 = 64
-                                 words wherever one stage fits (lists then read from
-                                 global memory); 32 = always 32 */
+    uint32_t group_tile_words;  /* dense group kernel tile: 0 or 64 = 64 words wherever
+                                 one stage fits shared memory (two stages where they
+                                 fit; the window's lists read from global memory when
+                                 they do not fit beside the stage), else 32; 32 =
+                                 always 32 */
 } abf_tuning;
 
 abf_status abf_get_tuning(const abf_index* index, abf_tuning* out);
