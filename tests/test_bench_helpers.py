@@ -59,6 +59,8 @@ def test_id_checksums_wrap_like_uint64():
     pos = np.arange(n, dtype=np.uint64)
     e1 = int(np.sum(ids.astype(np.uint64), dtype=np.uint64))
     e2 = int(np.sum(ids.astype(np.uint64) * pos, dtype=np.uint64))  # wraps modulo 2^64
-    assert sum(int(v) * i for i, v in enumerate(ids[::4096].tolist())) * 4096 > 1 << 64  # the sum does wrap
+    prod = ids.astype(np.uint64) * pos  # each term below 2^48: no wrap per term
+    exact = sum(int(c) for c in prod.reshape(-1, 1000).sum(axis=1, dtype=np.uint64))  # chunk sums below 2^58
+    assert exact >= 1 << 64 and e2 == exact % (1 << 64)  # the sum does wrap
     s1, s2 = b.id_checksums(torch.from_numpy(ids.view(np.int32).copy()), n, torch)
     assert (s1, s2) == (e1, e2)
