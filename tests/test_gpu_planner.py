@@ -144,3 +144,34 @@ def test_collect_labels_shapes(env):
     ix, qoff, qt = env["ix"], env["qoff"], env["qt"]
     t = P.collect_labels(ix, qoff[:11], qt[:qoff[10]])
     assert t.shape == (10, 3) and (t > 0).all()
+
+
+def test_fixed_rule_paths_match_host_restatement(env):
+    """Without a planner, ABF_PATH_AUTO takes the fixed rule in the plan
+    kernel; the path of every query equals planner.fixed_rule_choice (the
+    host restatement used to score the rule on labels)."""
+    import torch
+    ix, qoff, qt = env["ix"], env["qoff"], env["qt"]
+    n = qoff.size - 1
+    frac = P.touched_fraction(ix, qoff, qt)
+    mx = P.max_list_len(ix, qoff, qt)
+    fs = np.unique(frac)
+    tau = float((fs[len(fs) // 2] + fs[len(fs) // 2 + 1]) / 2)  # between two queries' fractions
+    hyb = int(np.median(mx[frac <= tau])) + 1
+    old = ix.tuning
+    ix.set_tuning(probe_min_fraction=tau, fixed_hybrid_min_len=hyb, probe_cap=64)
+    try:
+        n_words = (env["spec"].n_ads + 31) // 32
+        stride = (n_words + 3) // 4 * 4
+        ws = ix.workspace(n, int(qoff[-1]))
+        bms = torch.empty((n, stride), dtype=torch.int32, device="cuda")
+        dt, do = P.device_batch(qoff, qt)
+        ix.batch_run(ws, dt, do, n, bms, stride, path=ab.PATH_AUTO)
+        ws.check()
+        want = np.array(N.PLANNER_PATHS)[P.fixed_rule_choice(ix, qoff, qt, tau, hyb)]
+        got = ws.paths(n)
+        assert len(np.unique(want)) == 3  # the thresholds split the queries over all three paths
+        assert np.array_equal(got, want), (got, want)
+    finally:
+        ix.set_tuning(probe_min_fraction=old.probe_min_fraction, fixed_hybrid_min_len=old.fixed_hybrid_min_len,
+                      probe_cap=32)
